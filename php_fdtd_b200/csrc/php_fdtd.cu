@@ -1,0 +1,1131 @@
+/*
+ * php_fdtd.cu -- libphpfdtd: the C ABI of include/php_fdtd.h on one B200.
+ *
+ * Host side of the device path: derives every per-material and per-axis
+ * coefficient once (where the reference recomputes them per cell and step),
+ * lays the domain out in HBM (see php_kernels.cuh), records one CUDA graph
+ * per distinct step count and replays it, and serves the read-outs.
+ *
+ * Coefficients used by the strict mode are computed with the reference's
+ * expressions and evaluation order (this file is compiled with host FP
+ * contraction off), so the device sees the same doubles fdtd.c computes.
+ */
+#include "php_fdtd.h"
+#include "php_kernels.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+using namespace phpdev;
+
+namespace {
+
+constexpr int kMaxChunk = 256;      /* steps per recorded graph */
+constexpr int kProbeCap = 8192;     /* probe rows held on the device */
+constexpr double kEpsInf = 20.0;    /* EPS_INF, fdtd.c:202 */
+
+std::string g_create_error;
+
+struct DftPlane {
+    int comp, z, first, interval, nfreq, cast_f32;
+    std::vector<double> freq;
+    double* acc = nullptr; /* [nfreq][nx][ny][2] */
+    int nsamples = 0;
+    int in_off = 0;        /* offset of this plane's flag in a step-input row */
+};
+
+} // namespace
+
+struct php_ctx {
+    php_desc d{};
+    int prec = 0;
+    int nx = 0, ny = 0, nz = 0, nxp = 0, L = 0;
+    int64_t plane = 0, ncell_dev = 0;
+    int zchunk = 1;
+    int n3max = 0, namax_tpl = 0;
+    int64_t nslot = 0;
+    bool any_ade = false, any_atoms = false;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    uint64_t bytes = 0;
+    std::vector<void*> allocs;
+
+    /* device state */
+    void* f[9] = {};            /* field bases (plane 0) */
+    void* psi[12] = {};
+    uint8_t* mat = nullptr;
+    int32_t* slot = nullptr;
+    int64_t* slot_cell = nullptr;
+    int32_t* slot_n3 = nullptr;
+    void *P = nullptr, *Po = nullptr, *r = nullptr, *v = nullptr;
+    void* mc = nullptr;          /* MatCoef<R>[nmat] */
+    void* ion_coef = nullptr;
+    void* axis_tab[3][7] = {};   /* kappa b c kh kd ch cd per axis */
+    int32_t* axis_slot[3] = {};
+    double* step_in = nullptr;   /* [kMaxChunk][row] */
+    double* step_in_host = nullptr;
+    int step_row = 0;
+    void* scratch = nullptr;     /* plane gathers, diagnostics */
+    size_t scratch_bytes = 0;
+    void* host_stage = nullptr;  /* pinned */
+    size_t host_stage_bytes = 0;
+
+    /* host copies kept for reads */
+    std::vector<int> mat_natom, mat_ade;
+    std::vector<int32_t> slot_host_dummy;
+
+    /* sources */
+    std::vector<php_source_desc> src;
+    int64_t src_cell[kMaxSources] = {};
+    int32_t src_comp[kMaxSources] = {};
+    int nsrc_active = 0;
+    std::vector<int> src_active_index;
+
+    /* stepping */
+    int32_t t = 0;
+    std::map<int, cudaGraphExec_t> graphs;
+    int last_launches = 0;
+
+    /* probe */
+    bool probe = false;
+    int64_t probe_cf = 0, probe_slot = -1;
+    int probe_n3 = 0;
+    double* probe_rows = nullptr;
+    int32_t* probe_count = nullptr;
+
+    std::vector<DftPlane> dft;
+};
+
+/* ------------------------------------------------------------------ utils */
+
+static int fail(php_ctx* c, int code, const char* fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    else g_create_error = buf;
+    return code;
+}
+
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return fail(ctx, PHP_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                        __FILE__, __LINE__);                                                       \
+    } while (0)
+
+static int dalloc(php_ctx* ctx, void** p, size_t bytes)
+{
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return fail(ctx, PHP_ERR_OOM, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+    }
+    ctx->allocs.push_back(*p);
+    ctx->bytes += bytes;
+    e = cudaMemsetAsync(*p, 0, bytes, ctx->stream);
+    if (e != cudaSuccess) return fail(ctx, PHP_ERR_CUDA, "cudaMemset failed: %s", cudaGetErrorString(e));
+    return PHP_OK;
+}
+
+static size_t rsize(int prec) { return prec == PHP_PREC_FP32 ? sizeof(float) : sizeof(double); }
+
+/* --------------------------------------------------- coefficient derivation */
+
+/* Real part of inverse_dielectric_tensor (fdtd.c:555-625). */
+static int complex_inverse_re(const double* e, const double* ei, double* out)
+{
+    const double xx = e[0], xy = e[1], xz = e[2], yx = e[3], yy = e[4], yz = e[5], zx = e[6], zy = e[7], zz = e[8];
+    const double xxi = ei[0], xyi = ei[1], xzi = ei[2], yxi = ei[3], yyi = ei[4], yzi = ei[5], zxi = ei[6],
+                 zyi = ei[7], zzi = ei[8];
+    double det_real = xx * (yy * zz - yz * zy) - xy * (yx * zz - yz * zx) + xz * (yx * zy - yy * zx);
+    double det_imag = xxi * (yyi * zzi - yzi * zyi) - xyi * (yxi * zzi - yzi * zxi) + xzi * (yxi * zyi - yyi * zxi);
+    double det_magnitude = sqrt(det_real * det_real + det_imag * det_imag);
+    if (fabs(det_magnitude) < 1e-12) return -1;
+    double idr = det_real / (det_real * det_real + det_imag * det_imag);
+    double idi = -det_imag / (det_real * det_real + det_imag * det_imag);
+    out[0] = idr * (yy * zz - yz * zy) - idi * (yyi * zzi - yzi * zyi);
+    out[1] = idr * (xz * zy - xy * zz) - idi * (xzi * zyi - xyi * zzi);
+    out[2] = idr * (xy * yz - xz * yy) - idi * (xyi * yzi - xzi * yyi);
+    out[3] = idr * (yz * zx - yx * zz) - idi * (yzi * zxi - yxi * zzi);
+    out[4] = idr * (xx * zz - xz * zx) - idi * (xxi * zzi - xzi * zxi);
+    out[5] = idr * (xz * yx - xx * yz) - idi * (xzi * yxi - xxi * yzi);
+    out[6] = idr * (yx * zy - yy * zx) - idi * (yxi * zyi - yyi * zxi);
+    out[7] = idr * (xy * zx - xx * zy) - idi * (xyi * zxi - xxi * zyi);
+    out[8] = idr * (xx * yy - xy * yx) - idi * (xxi * yyi - xyi * yxi);
+    return 0;
+}
+
+/* 3x3 inverse by the adjugate (fdtd.c:205-258); -1 when |det| < 1e-12. */
+static int inverse3(const double m[3][3], double inv[3][3])
+{
+    double det = m[0][0] * (m[1][1] * m[2][2] - m[1][2] * m[2][1]) - m[0][1] * (m[1][0] * m[2][2] - m[1][2] * m[2][0]) +
+                 m[0][2] * (m[1][0] * m[2][1] - m[1][1] * m[2][0]);
+    if (fabs(det) < 1e-12) return -1;
+    double adj[3][3];
+    adj[0][0] = (m[1][1] * m[2][2] - m[1][2] * m[2][1]);
+    adj[0][1] = -(m[1][0] * m[2][2] - m[1][2] * m[2][0]);
+    adj[0][2] = (m[1][0] * m[2][1] - m[1][1] * m[2][0]);
+    adj[1][0] = -(m[0][1] * m[2][2] - m[0][2] * m[2][1]);
+    adj[1][1] = (m[0][0] * m[2][2] - m[0][2] * m[2][0]);
+    adj[1][2] = -(m[0][0] * m[2][1] - m[0][1] * m[2][0]);
+    adj[2][0] = (m[0][1] * m[1][2] - m[0][2] * m[1][1]);
+    adj[2][1] = -(m[0][0] * m[1][2] - m[0][2] * m[1][0]);
+    adj[2][2] = (m[0][0] * m[1][1] - m[0][1] * m[1][0]);
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) inv[i][j] = adj[j][i] / det;
+    return 0;
+}
+
+/* Double-precision per-material coefficients in the reference's order. */
+struct MatD {
+    int flags = 0, natom = 0;
+    double eps_inv[9] = {}, eps_im[9] = {};
+    double lf = 1.0, lt = 0.0, cs = 1.0, sn = 0.0;
+    double gp_inv[9] = {}, gm[9] = {}, wp2[9] = {};
+};
+
+static int derive_material(php_ctx* ctx, int id, const php_material_desc& m, MatD& o)
+{
+    const php_desc& d = ctx->d;
+    if (complex_inverse_re(m.eps_re, m.eps_im, o.eps_inv))
+        return fail(ctx, PHP_ERR_INPUT, "Error: Singular dielectric tensor! (material %d)", id);
+    memcpy(o.eps_im, m.eps_im, sizeof(o.eps_im));
+    /* fdtd.c:3414-3415 */
+    o.lf = 1.0 / (1.0 + m.sigma * d.dt / (2 * d.epsilon0));
+    o.lt = (m.sigma * d.dt / (2 * d.epsilon0)) * o.lf;
+    if (fabs(m.anglez) > 1e-10) {
+        o.flags |= kRotZ;
+        o.cs = cos(m.anglez);
+        o.sn = sin(m.anglez);
+    } else if (fabs(m.anglex) > 1e-10) {
+        o.flags |= kRotX;
+        o.cs = cos(-m.anglex);
+        o.sn = sin(-m.anglex);
+    }
+    if (m.use_ade != 0 && m.use_ade != 1) return fail(ctx, PHP_ERR_INPUT, "Error: use_ADE must be 0 or 1 (material %d)", id);
+    if (m.use_ade == 1) {
+        o.flags |= kAde;
+        const double f = d.source_frequency;
+        double epsr1[3][3], epsr1_inv[3][3], gama[3][3], gdt2p1[3][3], gdt2m1[3][3], gp_inv[3][3];
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) epsr1[a][b] = m.eps_re[a * 3 + b];
+        epsr1[0][0] = m.eps_re[0] - kEpsInf;
+        epsr1[1][1] = m.eps_re[4] - kEpsInf;
+        epsr1[2][2] = m.eps_re[8] - kEpsInf;
+        if (epsr1[0][0] >= 0 || epsr1[1][1] >= 0 || epsr1[2][2] >= 0)
+            return fail(ctx, PHP_ERR_INPUT, "Error: EPS_INF is too small for material %d", id);
+        if (inverse3(epsr1, epsr1_inv)) return fail(ctx, PHP_ERR_INPUT, "Error: epsr1 can not be inversed (material %d)", id);
+        const double* ei = m.eps_im;
+        /* fdtd.c:2490-2498 */
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++)
+                gama[a][b] = -(ei[a * 3 + 0] * epsr1_inv[0][b] + ei[a * 3 + 1] * epsr1_inv[1][b] + ei[a * 3 + 2] * epsr1_inv[2][b]) *
+                             f * 2.0 * M_PI;
+        /* fdtd.c:2499-2507 */
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++)
+                o.wp2[a * 3 + b] = -f * f * 4.0 * M_PI * M_PI * epsr1[a][b] +
+                                   f * 2.0 * M_PI * (gama[a][0] * ei[0 * 3 + b] + gama[a][1] * ei[1 * 3 + b] + gama[a][2] * ei[2 * 3 + b]);
+        /* fdtd.c:2508-2517 */
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) {
+                gdt2p1[a][b] = +gama[a][b] * d.dt / 2.0;
+                gdt2m1[a][b] = -gama[a][b] * d.dt / 2.0;
+                if (a == b) {
+                    gdt2p1[a][b] += 1.0;
+                    gdt2m1[a][b] += 1.0;
+                }
+            }
+        if (inverse3(gdt2p1, gp_inv)) return fail(ctx, PHP_ERR_INPUT, "Error: gdt2p1 can not be inversed (material %d)", id);
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) {
+                o.gp_inv[a * 3 + b] = gp_inv[a][b];
+                o.gm[a * 3 + b] = gdt2m1[a][b];
+            }
+    } else {
+        bool lossy = false;
+        for (int q = 0; q < 9; q++) lossy |= (m.eps_im[q] != 0.0);
+        if (lossy) o.flags |= kLossy;
+    }
+    if (m.natom < 0) return fail(ctx, PHP_ERR_INPUT, "negative natom (material %d)", id);
+    if (m.natom > 0) {
+        if (!m.qezv || !m.qezm || !m.dmm) return fail(ctx, PHP_ERR_INPUT, "material %d: natom > 0 needs QeZV, QeZM and DMM", id);
+        o.flags |= kAtoms;
+        o.natom = m.natom;
+    }
+    return PHP_OK;
+}
+
+template <typename R>
+static MatCoef<R> pack_material(const php_ctx* ctx, const MatD& s, int ion_off)
+{
+    MatCoef<R> o;
+    memset(&o, 0, sizeof(o));
+    o.flags = s.flags;
+    o.natom = s.natom;
+    o.ion_off = ion_off;
+    const php_desc& d = ctx->d;
+    const bool strict = ctx->prec == PHP_PREC_FP64_STRICT;
+    const double c1 = d.dt * d.source_frequency * 2.0 * 3.14159265;
+    const double e0dt2 = d.epsilon0 * d.dt * d.dt;
+    for (int q = 0; q < 9; q++) {
+        if (strict) {
+            o.eps_inv[q] = (R)s.eps_inv[q];
+            o.eps_im[q] = (R)s.eps_im[q];
+            o.wp2[q] = (R)s.wp2[q];
+        } else {
+            o.eps_inv[q] = (R)(s.eps_inv[q] * (s.lf * (1.0 - s.lt) / d.epsilon0));
+            o.eps_im[q] = (R)(s.eps_im[q] * c1 * d.epsilon0);
+            o.wp2[q] = (R)(s.wp2[q] * e0dt2);
+        }
+        o.gp_inv[q] = (R)s.gp_inv[q];
+        o.gm[q] = (R)s.gm[q];
+    }
+    o.lf = (R)s.lf;
+    o.lt = (R)s.lt;
+    o.cs = (R)s.cs;
+    o.sn = (R)s.sn;
+    o.ade_scale = (R)((1.0 - s.lt) / (d.epsilon0 * kEpsInf));
+    return o;
+}
+
+/* init_pml (fdtd.c:962-989) and the per-cell b, c of fdtd.c:3146-3151. */
+struct AxisD {
+    std::vector<int32_t> slot;
+    std::vector<double> kappa, b, c, kh, kd, ch, cd;
+};
+
+static void derive_axis(const php_desc& d, int n, double delta, bool is_z, AxisD& ax)
+{
+    const int L = d.pml_thickness;
+    ax.slot.assign(n, -1);
+    ax.kappa.assign(n, 1.0);
+    ax.b.assign(n, 1.0);
+    ax.c.assign(n, 0.0);
+    ax.kh.assign(n, 0.0);
+    ax.kd.assign(n, 0.0);
+    ax.ch.assign(n, 0.0);
+    ax.cd.assign(n, 0.0);
+    std::vector<double> sigma(L > 0 ? L : 0), kappa(L > 0 ? L : 0), alpha(L > 0 ? L : 0);
+    if (L > 0) {
+        double m = 3.0, kappa_max = 7.0, alpha_max = 0.05;
+        double eta0 = sqrt(d.mu0 / d.epsilon0);
+        double sigma_max = -(m + 1) * log(d.pml_reflection) / (2.0 * eta0 * delta * L);
+        for (int i = 0; i < L; i++) {
+            double r = (double)(L - i) / L;
+            sigma[i] = sigma_max * pow(r, m);
+            kappa[i] = 1.0 + (kappa_max - 1.0) * pow(r, m);
+            alpha[i] = alpha_max * (1.0 - r);
+        }
+    }
+    for (int i = 0; i < n; i++) {
+        int idx = -1, s = -1;
+        if (is_z) {
+            if (i < L || i >= n - L) {
+                idx = (i < L) ? i : n - 1 - i;
+                s = (i < L) ? i : L + idx;
+            }
+        } else if (L > 0 && i < L) {
+            idx = i;
+            s = i;
+        } else if (L > 0 && i >= n - L) {
+            idx = n - 1 - i;
+            s = L + idx;
+        }
+        double kap = 1.0, bb = 1.0, cc = 0.0;
+        if (idx >= 0) {
+            double sx = sigma[idx];
+            kap = kappa[idx];
+            double ax_ = alpha[idx];
+            double aw = sx / (kap * d.epsilon0) + ax_ / d.epsilon0;
+            bb = exp(-aw * d.dt);
+            cc = (aw > 1e-30) ? sx / (kap * kap * d.epsilon0) * (bb - 1.0) / aw : 0.0;
+        }
+        ax.slot[i] = s;
+        ax.kappa[i] = kap;
+        ax.b[i] = bb;
+        ax.c[i] = cc;
+        ax.kh[i] = d.dt / (d.mu0 * delta * kap);
+        ax.kd[i] = d.dt / (delta * kap);
+        ax.ch[i] = d.dt * cc / (d.mu0 * delta);
+        ax.cd[i] = d.dt * cc / delta;
+    }
+}
+
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+
+/* calculate_source_value, fdtd.c:1923-1947 */
+static double source_value(const php_source_desc* s, double time)
+{
+    if (time < s->start_time || time > s->end_time) return 0.0;
+    switch (s->type) {
+    case 0: return s->amplitude * exp(-pow((time - s->t0) / s->tau, 2));
+    case 1: return s->amplitude * sin(2 * M_PI * s->frequency * time);
+    case 2: {
+        double t_shift = time - s->t0;
+        double arg = M_PI * M_PI * s->frequency * s->frequency * t_shift * t_shift;
+        return s->amplitude * (1.0 - 2.0 * arg) * exp(-arg);
+    }
+    case 3: return s->amplitude * sin(2 * M_PI * s->frequency * time) * exp(-pow((time - s->t0) / s->tau, 2));
+    default: return 0.0;
+    }
+}
+
+/* ------------------------------------------------------------ kernel args */
+
+template <typename R>
+static StepArgs<R> make_args(php_ctx* ctx, int s_local)
+{
+    StepArgs<R> a;
+    memset(&a, 0, sizeof(a));
+    R* const* fp = reinterpret_cast<R* const*>(ctx->f);
+    a.f = Fields<R>{fp[0], fp[1], fp[2], fp[3], fp[4], fp[5], fp[6], fp[7], fp[8]};
+    R* const* pp = reinterpret_cast<R* const*>(ctx->psi);
+    a.psi = Psi<R>{pp[0], pp[1], pp[2], pp[3], pp[4], pp[5], pp[6], pp[7], pp[8], pp[9], pp[10], pp[11]};
+    AxisTab<R>* tabs[3] = {&a.tx, &a.ty, &a.tz};
+    for (int ax = 0; ax < 3; ax++) {
+        AxisTab<R>& t = *tabs[ax];
+        t.slot = ctx->axis_slot[ax];
+        t.kappa = (const R*)ctx->axis_tab[ax][0];
+        t.b = (const R*)ctx->axis_tab[ax][1];
+        t.c = (const R*)ctx->axis_tab[ax][2];
+        t.kh = (const R*)ctx->axis_tab[ax][3];
+        t.kd = (const R*)ctx->axis_tab[ax][4];
+        t.ch = (const R*)ctx->axis_tab[ax][5];
+        t.cd = (const R*)ctx->axis_tab[ax][6];
+    }
+    a.mat = ctx->mat;
+    a.slot = ctx->slot;
+    a.mc = (const MatCoef<R>*)ctx->mc;
+    a.ion_coef = (const R*)ctx->ion_coef;
+    a.P = (R*)ctx->P;
+    a.Po = (R*)ctx->Po;
+    a.r = (R*)ctx->r;
+    a.v = (R*)ctx->v;
+    a.nslot = ctx->nslot;
+    a.nx = ctx->nx;
+    a.ny = ctx->ny;
+    a.nz = ctx->nz;
+    a.nxp = ctx->nxp;
+    a.L = ctx->L;
+    a.zchunk = ctx->zchunk;
+    a.plane = ctx->plane;
+    const php_desc& d = ctx->d;
+    a.dt = d.dt;
+    a.dxs = d.dx;
+    a.dys = d.dy;
+    a.dzs = d.dz;
+    a.mu0 = d.mu0;
+    a.eps0 = d.epsilon0;
+    a.c1 = d.dt * d.source_frequency * 2.0 * 3.14159265;
+    a.e0dt2 = d.epsilon0 * d.dt * d.dt;
+    a.nsrc = ctx->nsrc_active;
+    for (int s = 0; s < ctx->nsrc_active; s++) {
+        a.src_cell[s] = ctx->src_cell[s];
+        a.src_comp[s] = ctx->src_comp[s];
+    }
+    a.src_val = ctx->step_in + (size_t)s_local * ctx->step_row;
+    return a;
+}
+
+template <typename R, bool STRICT, int NA>
+static void launch_step_t(php_ctx* ctx, int s_local, int& launches)
+{
+    StepArgs<R> a = make_args<R>(ctx, s_local);
+    dim3 block(kBlockX, 8, 1);
+    dim3 grid((ctx->nx + kBlockX - 1) / kBlockX, (ctx->ny + 7) / 8, (ctx->nz + ctx->zchunk - 1) / ctx->zchunk);
+    h_sweep<R, STRICT><<<grid, block, 0, ctx->stream>>>(a);
+    e_sweep<R, STRICT, NA><<<grid, block, 0, ctx->stream>>>(a);
+    launches += 2;
+    if (ctx->probe) {
+        R* const* fp = reinterpret_cast<R* const*>(ctx->f);
+        Fields<R> f{fp[0], fp[1], fp[2], fp[3], fp[4], fp[5], fp[6], fp[7], fp[8]};
+        const int threads = (9 + 2 * ctx->probe_n3 + 31) / 32 * 32;
+        probe_record_counted<R><<<1, threads, 0, ctx->stream>>>(
+            f, ctx->probe_cf, (const R*)ctx->r, (const R*)ctx->v, ctx->nslot, ctx->probe_slot, ctx->probe_n3,
+            ctx->probe_rows, ctx->probe_count, kProbeCap, 9 + 2 * ctx->probe_n3);
+        launches++;
+    }
+    for (auto& p : ctx->dft) {
+        R* const* fp = reinterpret_cast<R* const*>(ctx->f);
+        const int64_t n = (int64_t)ctx->nx * ctx->ny;
+        int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
+        dft_sample<R><<<blocks, 256, 0, ctx->stream>>>(fp[p.comp], (int64_t)p.z * ctx->plane, ctx->nx, ctx->ny, ctx->nxp,
+                                                       p.nfreq, p.cast_f32, ctx->step_in + (size_t)s_local * ctx->step_row,
+                                                       p.in_off, p.in_off + 1, p.acc);
+        launches++;
+    }
+}
+
+typedef void (*step_fn)(php_ctx*, int, int&);
+
+template <typename R, bool STRICT>
+static step_fn pick_na(int namax)
+{
+    switch (namax) {
+    case 0: return launch_step_t<R, STRICT, 0>;
+    case 2: return launch_step_t<R, STRICT, 2>;
+    case 4: return launch_step_t<R, STRICT, 4>;
+    case 8: return launch_step_t<R, STRICT, 8>;
+    case 16: return launch_step_t<R, STRICT, 16>;
+    default: return launch_step_t<R, STRICT, 64>;
+    }
+}
+
+static step_fn pick_step(const php_ctx* ctx)
+{
+    if (ctx->prec == PHP_PREC_FP64_STRICT) return pick_na<double, true>(ctx->namax_tpl);
+    if (ctx->prec == PHP_PREC_FP64) return pick_na<double, false>(ctx->namax_tpl);
+    return pick_na<float, false>(ctx->namax_tpl);
+}
+
+/* --------------------------------------------------------------- creation */
+
+template <typename R>
+static int upload_tables(php_ctx* ctx, const std::vector<MatD>& mats, const std::vector<int>& ion_off,
+                         const std::vector<double>& ion_coef, const AxisD* axes)
+{
+    std::vector<MatCoef<R>> mc(mats.size());
+    for (size_t i = 0; i < mats.size(); i++) mc[i] = pack_material<R>(ctx, mats[i], ion_off[i]);
+    int rc = dalloc(ctx, &ctx->mc, mc.size() * sizeof(MatCoef<R>));
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(ctx->mc, mc.data(), mc.size() * sizeof(MatCoef<R>), cudaMemcpyHostToDevice, ctx->stream));
+    std::vector<R> ic(ion_coef.size() ? ion_coef.size() : 1);
+    for (size_t i = 0; i < ion_coef.size(); i++) ic[i] = (R)ion_coef[i];
+    rc = dalloc(ctx, &ctx->ion_coef, ic.size() * sizeof(R));
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(ctx->ion_coef, ic.data(), ic.size() * sizeof(R), cudaMemcpyHostToDevice, ctx->stream));
+    for (int ax = 0; ax < 3; ax++) {
+        const AxisD& A = axes[ax];
+        const std::vector<double>* cols[7] = {&A.kappa, &A.b, &A.c, &A.kh, &A.kd, &A.ch, &A.cd};
+        for (int q = 0; q < 7; q++) {
+            std::vector<R> h(cols[q]->size());
+            for (size_t i = 0; i < h.size(); i++) h[i] = (R)(*cols[q])[i];
+            rc = dalloc(ctx, &ctx->axis_tab[ax][q], h.size() * sizeof(R));
+            if (rc) return rc;
+            CK(cudaMemcpyAsync(ctx->axis_tab[ax][q], h.data(), h.size() * sizeof(R), cudaMemcpyHostToDevice, ctx->stream));
+        }
+        rc = dalloc(ctx, (void**)&ctx->axis_slot[ax], A.slot.size() * sizeof(int32_t));
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(ctx->axis_slot[ax], A.slot.data(), A.slot.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                           ctx->stream));
+    }
+    /* host tables must stay alive until the copies finish */
+    CK(cudaStreamSynchronize(ctx->stream));
+    return PHP_OK;
+}
+
+static void ctx_free(php_ctx* ctx)
+{
+    if (!ctx) return;
+    for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.second);
+    ctx->graphs.clear();
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (void* p : ctx->allocs) cudaFree(p);
+    ctx->allocs.clear();
+    if (ctx->host_stage) cudaFreeHost(ctx->host_stage);
+    if (ctx->step_in_host) cudaFreeHost(ctx->step_in_host);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+static int create_impl(const php_desc* desc, php_ctx* ctx)
+{
+    const php_desc& d = *desc;
+    if (d.abi_version != PHP_ABI_VERSION) return fail(ctx, PHP_ERR_INPUT, "abi_version %d, library %d", d.abi_version, PHP_ABI_VERSION);
+    if (d.nx < 2 || d.ny < 2 || d.nz < 1) return fail(ctx, PHP_ERR_INPUT, "grid %dx%dx%d too small", d.nx, d.ny, d.nz);
+    if (!(d.dt > 0) || !(d.dx > 0) || !(d.dy > 0) || !(d.dz > 0))
+        return fail(ctx, PHP_ERR_INPUT, "dt and cell sizes must be positive");
+    if (d.precision < 0 || d.precision > 2) return fail(ctx, PHP_ERR_INPUT, "unknown precision %d", d.precision);
+    if (d.pml_thickness < 0) return fail(ctx, PHP_ERR_INPUT, "negative pml_thickness");
+    if (d.num_materials < 1 || d.num_materials > 256 || !d.materials)
+        return fail(ctx, PHP_ERR_INPUT, "num_materials must be 1..256 (got %d)", d.num_materials);
+    if (!d.medium) return fail(ctx, PHP_ERR_INPUT, "medium is NULL");
+    if (d.num_sources < 0 || (d.num_sources > 0 && !d.sources)) return fail(ctx, PHP_ERR_INPUT, "bad sources");
+    ctx->d = d;
+    ctx->prec = d.precision;
+    ctx->nx = d.nx;
+    ctx->ny = d.ny;
+    ctx->nz = d.nz;
+    ctx->nxp = (d.nx + 31) / 32 * 32;
+    ctx->L = d.pml_thickness;
+    ctx->plane = (int64_t)ctx->nxp * d.ny;
+    ctx->ncell_dev = ctx->plane * d.nz;
+
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(ctx, PHP_ERR_NODEVICE, "no CUDA device visible");
+    if (d.device < 0 || d.device >= ndev) return fail(ctx, PHP_ERR_INPUT, "device %d not present", d.device);
+    CK(cudaSetDevice(d.device));
+    CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+
+    /* materials */
+    std::vector<MatD> mats(d.num_materials);
+    std::vector<int> ion_off(d.num_materials, 0);
+    std::vector<double> ion_coef;
+    for (int i = 0; i < d.num_materials; i++) {
+        int rc = derive_material(ctx, i, d.materials[i], mats[i]);
+        if (rc) return rc;
+        if (mats[i].natom > 0) {
+            const int N = mats[i].natom;
+            ion_off[i] = (int)ion_coef.size();
+            ion_coef.insert(ion_coef.end(), d.materials[i].qezv, d.materials[i].qezv + 9 * N);
+            ion_coef.insert(ion_coef.end(), d.materials[i].qezm, d.materials[i].qezm + 9 * N);
+            ion_coef.insert(ion_coef.end(), d.materials[i].dmm, d.materials[i].dmm + 9 * N * N);
+        }
+        ctx->mat_natom.push_back(mats[i].natom);
+        ctx->mat_ade.push_back(mats[i].flags & kAde ? 1 : 0);
+    }
+
+    /* medium census, slots, device material map */
+    const int nx = d.nx, ny = d.ny, nz = d.nz, nxp = ctx->nxp;
+    std::vector<uint8_t> mat_dev((size_t)ctx->ncell_dev, 0);
+    std::vector<int32_t> slot_dev;
+    std::vector<int64_t> slot_cell;
+    std::vector<int32_t> slot_n3;
+    int n3max = 0;
+    for (int k = 0; k < nz; k++)
+        for (int j = 0; j < ny; j++)
+            for (int i = 0; i < nx; i++) {
+                int32_t id = d.medium[((size_t)i * ny + j) * nz + k];
+                if (id < 0 || id >= d.num_materials)
+                    return fail(ctx, PHP_ERR_INPUT, "medium id %d at (%d,%d,%d) outside the material table (0..%d)", id, i, j,
+                                k, d.num_materials - 1);
+                const int64_t c = ((int64_t)k * ny + j) * nxp + i;
+                mat_dev[c] = (uint8_t)id;
+                if (mats[id].flags & (kAde | kAtoms)) {
+                    slot_cell.push_back(c);
+                    slot_n3.push_back(3 * mats[id].natom);
+                    n3max = std::max(n3max, 3 * mats[id].natom);
+                    if (mats[id].flags & kAde) ctx->any_ade = true;
+                    if (mats[id].flags & kAtoms) ctx->any_atoms = true;
+                }
+            }
+    ctx->nslot = (int64_t)slot_cell.size();
+    ctx->n3max = n3max;
+    const int namax = n3max / 3;
+    ctx->namax_tpl = namax == 0 ? 0 : namax <= 2 ? 2 : namax <= 4 ? 4 : namax <= 8 ? 8 : namax <= 16 ? 16 : 64;
+    if (namax > 64) return fail(ctx, PHP_ERR_UNSUPPORTED, "natom %d above the supported 64", namax);
+
+    /* sources */
+    if (d.num_sources > kMaxSources) return fail(ctx, PHP_ERR_UNSUPPORTED, "at most %d sources", kMaxSources);
+    ctx->src.assign(d.sources, d.sources + d.num_sources);
+    for (int s = 0; s < d.num_sources; s++) {
+        const php_source_desc& S = d.sources[s];
+        /* fdtd.c:3375-3393: sources outside the grid or with an unknown
+         * component are skipped (their value still goes to source.txt) */
+        if (S.x < 0 || S.x >= nx || S.y < 0 || S.y >= ny || S.z < 0 || S.z >= nz) continue;
+        int comp = S.component == 'x' ? 0 : S.component == 'y' ? 1 : S.component == 'z' ? 2 : -1;
+        if (comp < 0) continue;
+        ctx->src_cell[ctx->nsrc_active] = ((int64_t)S.z * ny + S.y) * nxp + S.x;
+        ctx->src_comp[ctx->nsrc_active] = comp;
+        ctx->src_active_index.push_back(s);
+        ctx->nsrc_active++;
+    }
+
+    /* z chunking: enough blocks to cover 148 SMs several times over */
+    {
+        const int tiles = ((nx + kBlockX - 1) / kBlockX) * ((ny + 7) / 8);
+        int nchunks = (int)std::max<int64_t>(1, std::min<int64_t>(nz, (2048 + tiles - 1) / tiles));
+        ctx->zchunk = d.z_chunk > 0 ? d.z_chunk : (nz + nchunks - 1) / nchunks;
+    }
+
+    /* allocations */
+    const size_t rs = rsize(ctx->prec);
+    const size_t field_bytes = (size_t)ctx->plane * (nz + 2) * rs;
+    for (int q = 0; q < 9; q++) {
+        void* p;
+        int rc = dalloc(ctx, &p, field_bytes);
+        if (rc) return rc;
+        ctx->f[q] = (char*)p + (size_t)ctx->plane * rs; /* plane 0; plane -1 is the low halo */
+    }
+    const int L = ctx->L;
+    const size_t xs = (size_t)nz * ny * 2 * L, ys = (size_t)nz * 2 * L * nxp, zs = (size_t)2 * L * ny * nxp;
+    const size_t psz[12] = {xs, xs, ys, ys, zs, zs, xs, xs, ys, ys, zs, zs};
+    for (int q = 0; q < 12; q++) {
+        int rc = dalloc(ctx, &ctx->psi[q], psz[q] * rs);
+        if (rc) return rc;
+    }
+    int rc = dalloc(ctx, (void**)&ctx->mat, mat_dev.size());
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(ctx->mat, mat_dev.data(), mat_dev.size(), cudaMemcpyHostToDevice, ctx->stream));
+    if (ctx->nslot > 0) {
+        slot_dev.assign((size_t)ctx->ncell_dev, -1);
+        for (int64_t s = 0; s < ctx->nslot; s++) slot_dev[slot_cell[s]] = (int32_t)s;
+        rc = dalloc(ctx, (void**)&ctx->slot, slot_dev.size() * sizeof(int32_t));
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(ctx->slot, slot_dev.data(), slot_dev.size() * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
+        rc = dalloc(ctx, (void**)&ctx->slot_cell, slot_cell.size() * sizeof(int64_t));
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(ctx->slot_cell, slot_cell.data(), slot_cell.size() * sizeof(int64_t), cudaMemcpyHostToDevice,
+                           ctx->stream));
+        rc = dalloc(ctx, (void**)&ctx->slot_n3, slot_n3.size() * sizeof(int32_t));
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(ctx->slot_n3, slot_n3.data(), slot_n3.size() * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    if (ctx->any_ade) {
+        if ((rc = dalloc(ctx, &ctx->P, 3 * (size_t)ctx->nslot * rs))) return rc;
+        if ((rc = dalloc(ctx, &ctx->Po, 3 * (size_t)ctx->nslot * rs))) return rc;
+    }
+    if (ctx->any_atoms) {
+        if ((rc = dalloc(ctx, &ctx->r, (size_t)n3max * ctx->nslot * rs))) return rc;
+        if ((rc = dalloc(ctx, &ctx->v, (size_t)n3max * ctx->nslot * rs))) return rc;
+    }
+
+    AxisD axes[3];
+    derive_axis(d, nx, d.dx, false, axes[0]);
+    derive_axis(d, ny, d.dy, false, axes[1]);
+    derive_axis(d, nz, d.dz, true, axes[2]);
+    if (ctx->prec == PHP_PREC_FP32) rc = upload_tables<float>(ctx, mats, ion_off, ion_coef, axes);
+    else rc = upload_tables<double>(ctx, mats, ion_off, ion_coef, axes);
+    if (rc) return rc;
+
+    /* per-step inputs, scratch, staging */
+    ctx->step_row = std::max(1, ctx->nsrc_active);
+    if ((rc = dalloc(ctx, (void**)&ctx->step_in, (size_t)kMaxChunk * ctx->step_row * sizeof(double)))) return rc;
+    CK(cudaMallocHost((void**)&ctx->step_in_host, (size_t)kMaxChunk * ctx->step_row * sizeof(double)));
+    const size_t maxplane = std::max({(size_t)nx * ny, (size_t)ny * nz, (size_t)nx * nz});
+    ctx->scratch_bytes = std::max(maxplane * sizeof(double), (size_t)4096 * sizeof(DiagPartial));
+    if ((rc = dalloc(ctx, &ctx->scratch, ctx->scratch_bytes))) return rc;
+    ctx->host_stage_bytes = ctx->scratch_bytes;
+    CK(cudaMallocHost(&ctx->host_stage, ctx->host_stage_bytes));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return PHP_OK;
+}
+
+/* ---------------------------------------------------------------- stepping */
+
+static int ensure_graph(php_ctx* ctx, int n, cudaGraphExec_t* out)
+{
+    auto it = ctx->graphs.find(n);
+    if (it != ctx->graphs.end()) {
+        *out = it->second;
+        return PHP_OK;
+    }
+    step_fn fn = pick_step(ctx);
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    int launches = 0;
+    for (int s = 0; s < n; s++) fn(ctx, s, launches);
+    cudaError_t le = cudaGetLastError();
+    cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
+    if (le != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return fail(ctx, PHP_ERR_CUDA, "kernel launch during capture failed: %s", cudaGetErrorString(le));
+    }
+    if (ce != cudaSuccess) return fail(ctx, PHP_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+    cudaGraphExec_t ge = nullptr;
+    cudaError_t ie = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) return fail(ctx, PHP_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ie));
+    ctx->graphs[n] = ge;
+    *out = ge;
+    return PHP_OK;
+}
+
+static void drop_graphs(php_ctx* ctx)
+{
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.second);
+    ctx->graphs.clear();
+}
+
+static int relayout_step_inputs(php_ctx* ctx)
+{
+    int row = std::max(1, ctx->nsrc_active);
+    for (auto& p : ctx->dft) {
+        p.in_off = row;
+        row += 1 + 2 * p.nfreq;
+    }
+    if (row == ctx->step_row) return PHP_OK;
+    drop_graphs(ctx);
+    /* the old buffers stay in the allocation list until destroy */
+    ctx->step_row = row;
+    int rc = dalloc(ctx, (void**)&ctx->step_in, (size_t)kMaxChunk * row * sizeof(double));
+    if (rc) return rc;
+    if (ctx->step_in_host) cudaFreeHost(ctx->step_in_host);
+    ctx->step_in_host = nullptr;
+    CK(cudaMallocHost((void**)&ctx->step_in_host, (size_t)kMaxChunk * row * sizeof(double)));
+    return PHP_OK;
+}
+
+template <typename R>
+static void launch_gather_plane(php_ctx* ctx, int comp, int axis, int pos, bool f32)
+{
+    R* const* fp = reinterpret_cast<R* const*>(ctx->f);
+    Fields<R> f{fp[0], fp[1], fp[2], fp[3], fp[4], fp[5], fp[6], fp[7], fp[8]};
+    if (f32) gather_plane<R, float><<<296, 256, 0, ctx->stream>>>(f, comp, axis, pos, ctx->nx, ctx->ny, ctx->nz, ctx->nxp, (float*)ctx->scratch);
+    else gather_plane<R, double><<<296, 256, 0, ctx->stream>>>(f, comp, axis, pos, ctx->nx, ctx->ny, ctx->nz, ctx->nxp, (double*)ctx->scratch);
+}
+
+/* ------------------------------------------------------------- public API */
+
+extern "C" {
+
+int php_create(const php_desc* desc, php_ctx** out)
+{
+    if (!desc || !out) return fail(nullptr, PHP_ERR_INPUT, "null argument");
+    *out = nullptr;
+    php_ctx* ctx = new (std::nothrow) php_ctx();
+    if (!ctx) return fail(nullptr, PHP_ERR_OOM, "host allocation failed");
+    int rc = create_impl(desc, ctx);
+    if (rc) {
+        g_create_error = ctx->err;
+        ctx_free(ctx);
+        return rc;
+    }
+    *out = ctx;
+    return PHP_OK;
+}
+
+int php_destroy(php_ctx* ctx)
+{
+    ctx_free(ctx);
+    return PHP_OK;
+}
+
+const char* php_last_error(const php_ctx* ctx)
+{
+    if (!ctx) return g_create_error.c_str();
+    return ctx->err.c_str();
+}
+
+int php_step(php_ctx* ctx, int32_t nsteps)
+{
+    if (!ctx) return PHP_ERR_INPUT;
+    if (nsteps < 0) return fail(ctx, PHP_ERR_INPUT, "negative step count");
+    ctx->last_launches = 0;
+    const double dt = ctx->d.dt;
+    while (nsteps > 0) {
+        const int n = std::min(nsteps, kMaxChunk);
+        /* wait until the previous chunk has consumed the staging buffer */
+        CK(cudaStreamSynchronize(ctx->stream));
+        double* h = ctx->step_in_host;
+        for (int s = 0; s < n; s++) {
+            const int t = ctx->t + s;
+            double* row = h + (size_t)s * ctx->step_row;
+            const double current_time = t * dt; /* fdtd.c:3117 */
+            for (int q = 0; q < ctx->nsrc_active; q++)
+                row[q] = source_value(&ctx->src[ctx->src_active_index[q]], current_time);
+            for (auto& p : ctx->dft) {
+                const bool take = t >= p.first && ((t - p.first) % p.interval) == 0;
+                row[p.in_off] = take ? 1.0 : 0.0;
+                for (int f = 0; f < p.nfreq; f++) {
+                    const double ph = -2.0 * M_PI * p.freq[f] * (t * dt);
+                    row[p.in_off + 1 + 2 * f] = take ? cos(ph) : 0.0;
+                    row[p.in_off + 2 + 2 * f] = take ? sin(ph) : 0.0;
+                }
+                if (take) p.nsamples++;
+            }
+        }
+        CK(cudaMemcpyAsync(ctx->step_in, h, (size_t)n * ctx->step_row * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        cudaGraphExec_t g;
+        int rc = ensure_graph(ctx, n, &g);
+        if (rc) return rc;
+        CK(cudaGraphLaunch(g, ctx->stream));
+        ctx->last_launches += n * (2 + (ctx->probe ? 1 : 0) + (int)ctx->dft.size());
+        ctx->t += n;
+        nsteps -= n;
+    }
+    return PHP_OK;
+}
+
+int php_sync(php_ctx* ctx)
+{
+    if (!ctx) return PHP_ERR_INPUT;
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaGetLastError());
+    return PHP_OK;
+}
+
+int php_get_step(const php_ctx* ctx, int32_t* t)
+{
+    if (!ctx || !t) return PHP_ERR_INPUT;
+    *t = ctx->t;
+    return PHP_OK;
+}
+
+static int read_slice_impl(php_ctx* ctx, int32_t comp, char axis, int32_t position, void* out, bool f32)
+{
+    if (!ctx || !out) return PHP_ERR_INPUT;
+    if (comp < 0 || comp > 9) return fail(ctx, PHP_ERR_INPUT, "bad component %d", comp);
+    int ax, pos;
+    size_t n;
+    if (axis == 'z') {
+        if (position < 0 || position >= ctx->nz) return fail(ctx, PHP_ERR_INPUT, "Error: No process contains slice z=%d", position);
+        ax = 0;
+        pos = position + 1; /* fdtd.c:1029 with the halo already in the pointers (fdtd.c:274) */
+        n = (size_t)ctx->nx * ctx->ny;
+    } else if (axis == 'x') {
+        if (position < 0 || position >= ctx->nx)
+            return fail(ctx, PHP_ERR_INPUT, "Error: Invalid x slice position %d (range: 0-%d)", position, ctx->nx - 1);
+        ax = 1;
+        pos = position;
+        n = (size_t)ctx->ny * ctx->nz;
+    } else if (axis == 'y') {
+        if (position < 0 || position >= ctx->ny)
+            return fail(ctx, PHP_ERR_INPUT, "Error: Invalid y slice position %d (range: 0-%d)", position, ctx->ny - 1);
+        ax = 2;
+        pos = position;
+        n = (size_t)ctx->nx * ctx->nz;
+    } else {
+        return fail(ctx, PHP_ERR_INPUT, "Error: Invalid slice axis '%c'. Must be 'x', 'y', or 'z'.", axis);
+    }
+    if (ctx->prec == PHP_PREC_FP32) launch_gather_plane<float>(ctx, comp, ax, pos, f32);
+    else launch_gather_plane<double>(ctx, comp, ax, pos, f32);
+    CK(cudaGetLastError());
+    const size_t bytes = n * (f32 ? sizeof(float) : sizeof(double));
+    CK(cudaMemcpyAsync(ctx->host_stage, ctx->scratch, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    memcpy(out, ctx->host_stage, bytes);
+    return PHP_OK;
+}
+
+int php_read_slice(php_ctx* ctx, int32_t comp, char axis, int32_t position, float* out)
+{
+    return read_slice_impl(ctx, comp, axis, position, out, true);
+}
+
+int php_read_slice_f64(php_ctx* ctx, int32_t comp, char axis, int32_t position, double* out)
+{
+    return read_slice_impl(ctx, comp, axis, position, out, false);
+}
+
+int php_read_volume(php_ctx* ctx, int32_t comp, double* out)
+{
+    if (!ctx || !out) return PHP_ERR_INPUT;
+    if (comp < 0 || comp > 8) return fail(ctx, PHP_ERR_INPUT, "bad component %d", comp);
+    const size_t n = (size_t)ctx->nx * ctx->ny * ctx->nz;
+    void* dbuf = nullptr;
+    CK(cudaMallocAsync(&dbuf, n * sizeof(double), ctx->stream));
+    if (ctx->prec == PHP_PREC_FP32)
+        gather_volume<float><<<592, 256, 0, ctx->stream>>>((const float*)ctx->f[comp], ctx->nx, ctx->ny, ctx->nz, ctx->nxp, (double*)dbuf);
+    else
+        gather_volume<double><<<592, 256, 0, ctx->stream>>>((const double*)ctx->f[comp], ctx->nx, ctx->ny, ctx->nz, ctx->nxp, (double*)dbuf);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, dbuf, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaFreeAsync(dbuf, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return PHP_OK;
+}
+
+int php_read_point(php_ctx* ctx, int32_t i, int32_t j, int32_t k, double* out9)
+{
+    if (!ctx || !out9) return PHP_ERR_INPUT;
+    if (i < 0 || i >= ctx->nx || j < 0 || j >= ctx->ny || k < -1 || k > ctx->nz)
+        return fail(ctx, PHP_ERR_INPUT, "point (%d,%d,%d) outside the grid", i, j, k);
+    const int64_t c = ((int64_t)k * ctx->ny + j) * ctx->nxp + i;
+    const size_t rs = rsize(ctx->prec);
+    char* stage = (char*)ctx->host_stage;
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int q = 0; q < 9; q++)
+        CK(cudaMemcpyAsync(stage + q * rs, (const char*)ctx->f[q] + c * (int64_t)rs, rs, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int q = 0; q < 9; q++) out9[q] = rs == 4 ? (double)((float*)stage)[q] : ((double*)stage)[q];
+    return PHP_OK;
+}
+
+int php_read_cell_state(php_ctx* ctx, int32_t i, int32_t j, int32_t k, int32_t* natom, double* r, double* v,
+                        double* p_ade, double* p_ade_old)
+{
+    if (!ctx) return PHP_ERR_INPUT;
+    if (i < 0 || i >= ctx->nx || j < 0 || j >= ctx->ny || k < 0 || k >= ctx->nz)
+        return fail(ctx, PHP_ERR_INPUT, "cell (%d,%d,%d) outside the grid", i, j, k);
+    const int64_t c = ((int64_t)k * ctx->ny + j) * ctx->nxp + i;
+    CK(cudaStreamSynchronize(ctx->stream));
+    uint8_t mid = 0;
+    CK(cudaMemcpy(&mid, ctx->mat + c, 1, cudaMemcpyDeviceToHost));
+    const int na = ctx->mat_natom[mid];
+    if (natom) *natom = na;
+    int32_t s = -1;
+    if (ctx->slot) CK(cudaMemcpy(&s, ctx->slot + c, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    const size_t rs = rsize(ctx->prec);
+    auto fetch = [&](void* base, int q, double* dst) -> int {
+        char tmp[8];
+        cudaError_t e = cudaMemcpy(tmp, (const char*)base + ((int64_t)q * ctx->nslot + s) * (int64_t)rs, rs, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return fail(ctx, PHP_ERR_CUDA, "cudaMemcpy: %s", cudaGetErrorString(e));
+        *dst = rs == 4 ? (double)*(float*)tmp : *(double*)tmp;
+        return PHP_OK;
+    };
+    for (int q = 0; q < 3 * na; q++) {
+        if (r) { int rc = fetch(ctx->r, q, &r[q]); if (rc) return rc; }
+        if (v) { int rc = fetch(ctx->v, q, &v[q]); if (rc) return rc; }
+    }
+    if (ctx->mat_ade[mid] && s >= 0) {
+        for (int q = 0; q < 3; q++) {
+            if (p_ade) { int rc = fetch(ctx->P, q, &p_ade[q]); if (rc) return rc; }
+            if (p_ade_old) { int rc = fetch(ctx->Po, q, &p_ade_old[q]); if (rc) return rc; }
+        }
+    } else {
+        for (int q = 0; q < 3; q++) {
+            if (p_ade) p_ade[q] = 0.0;
+            if (p_ade_old) p_ade_old[q] = 0.0;
+        }
+    }
+    return PHP_OK;
+}
+
+int php_diagnostics(php_ctx* ctx, php_diag* out)
+{
+    if (!ctx || !out) return PHP_ERR_INPUT;
+    const int blocks = 148 * 4;
+    DiagPartial* part = (DiagPartial*)ctx->scratch;
+    DiagPartial* fin = part + blocks;
+    if (ctx->prec == PHP_PREC_FP32) {
+        float* const* fp = reinterpret_cast<float* const*>(ctx->f);
+        Fields<float> f{fp[0], fp[1], fp[2], fp[3], fp[4], fp[5], fp[6], fp[7], fp[8]};
+        diag_pass1<float><<<blocks, 256, 0, ctx->stream>>>(f, ctx->nx, ctx->ny, ctx->nz, ctx->nxp, (const float*)ctx->r,
+                                                           ctx->any_atoms ? ctx->nslot : 0, ctx->slot_cell, ctx->slot_n3,
+                                                           std::max(ctx->n3max, 1), part);
+    } else {
+        double* const* fp = reinterpret_cast<double* const*>(ctx->f);
+        Fields<double> f{fp[0], fp[1], fp[2], fp[3], fp[4], fp[5], fp[6], fp[7], fp[8]};
+        diag_pass1<double><<<blocks, 256, 0, ctx->stream>>>(f, ctx->nx, ctx->ny, ctx->nz, ctx->nxp, (const double*)ctx->r,
+                                                            ctx->any_atoms ? ctx->nslot : 0, ctx->slot_cell, ctx->slot_n3,
+                                                            std::max(ctx->n3max, 1), part);
+    }
+    diag_pass2<<<1, 256, 0, ctx->stream>>>(part, blocks, fin);
+    CK(cudaGetLastError());
+    DiagPartial h;
+    CK(cudaMemcpyAsync(ctx->host_stage, fin, sizeof(DiagPartial), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    memcpy(&h, ctx->host_stage, sizeof(h));
+    out->max_e = h.max_e;
+    out->max_ex = h.max_ex;
+    out->max_r = h.max_r;
+    if (h.max_r > 0.0 && h.key_r != INT64_MAX) {
+        const int64_t n3 = std::max(ctx->n3max, 1);
+        int64_t cell = h.key_r / n3;
+        const int q = (int)(h.key_r % n3);
+        out->argmax_r[2] = (int)(cell % ctx->nz);
+        cell /= ctx->nz;
+        out->argmax_r[1] = (int)(cell % ctx->ny);
+        out->argmax_r[0] = (int)(cell / ctx->ny);
+        out->argmax_r[3] = q / 3;
+        out->argmax_r[4] = q % 3;
+    } else {
+        for (int q = 0; q < 5; q++) out->argmax_r[q] = -1;
+    }
+    return PHP_OK;
+}
+
+int php_probe_set(php_ctx* ctx, int32_t i, int32_t j, int32_t k_field, int32_t k_atom)
+{
+    if (!ctx) return PHP_ERR_INPUT;
+    if (i < 0 || i >= ctx->nx || j < 0 || j >= ctx->ny || k_field < -1 || k_field > ctx->nz || k_atom < 0 || k_atom >= ctx->nz)
+        return fail(ctx, PHP_ERR_INPUT, "probe (%d,%d,%d/%d) outside the grid", i, j, k_field, k_atom);
+    drop_graphs(ctx);
+    ctx->probe_cf = ((int64_t)k_field * ctx->ny + j) * ctx->nxp + i;
+    const int64_t ca = ((int64_t)k_atom * ctx->ny + j) * ctx->nxp + i;
+    uint8_t mid = 0;
+    CK(cudaMemcpy(&mid, ctx->mat + ca, 1, cudaMemcpyDeviceToHost));
+    ctx->probe_n3 = 3 * ctx->mat_natom[mid];
+    int32_t s = -1;
+    if (ctx->slot) CK(cudaMemcpy(&s, ctx->slot + ca, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    ctx->probe_slot = s;
+    if (ctx->probe_n3 == 0) ctx->probe_slot = 0;
+    if (!ctx->probe_rows) {
+        int rc = dalloc(ctx, (void**)&ctx->probe_rows, (size_t)kProbeCap * (9 + 2 * std::max(ctx->n3max, 1)) * sizeof(double));
+        if (rc) return rc;
+        rc = dalloc(ctx, (void**)&ctx->probe_count, 2 * sizeof(int32_t));
+        if (rc) return rc;
+    }
+    CK(cudaMemsetAsync(ctx->probe_count, 0, 2 * sizeof(int32_t), ctx->stream));
+    ctx->probe = true;
+    return PHP_OK;
+}
+
+int php_probe_read(php_ctx* ctx, double* rows, int32_t max_rows, int32_t* nrows, int32_t* row_len)
+{
+    if (!ctx || !nrows) return PHP_ERR_INPUT;
+    if (!ctx->probe) return fail(ctx, PHP_ERR_STATE, "no probe set");
+    int32_t cnt[2];
+    CK(cudaMemcpyAsync(cnt, ctx->probe_count, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const int rl = 9 + 2 * ctx->probe_n3;
+    if (row_len) *row_len = rl;
+    if (cnt[1]) return fail(ctx, PHP_ERR_STATE, "probe buffer overflowed (more than %d rows between reads)", kProbeCap);
+    if (cnt[0] > max_rows) return fail(ctx, PHP_ERR_STATE, "%d probe rows pending, buffer holds %d", cnt[0], max_rows);
+    if (cnt[0] > 0 && rows)
+        CK(cudaMemcpyAsync(rows, ctx->probe_rows, (size_t)cnt[0] * rl * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemsetAsync(ctx->probe_count, 0, 2 * sizeof(int32_t), ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    *nrows = cnt[0];
+    return PHP_OK;
+}
+
+int php_dft_add(php_ctx* ctx, int32_t comp, int32_t z_plane, int32_t first_step, int32_t sample_interval, int32_t nfreq,
+                const double* freq_hz, int32_t cast_f32, int32_t* id)
+{
+    if (!ctx || !freq_hz || !id) return PHP_ERR_INPUT;
+    if (comp < 0 || comp > 8) return fail(ctx, PHP_ERR_INPUT, "DFT component must be 0..8");
+    if (z_plane < -1 || z_plane > ctx->nz) return fail(ctx, PHP_ERR_INPUT, "DFT plane %d outside -1..nz", z_plane);
+    if (sample_interval < 1 || nfreq < 1 || nfreq > 64 || first_step < 0) return fail(ctx, PHP_ERR_INPUT, "bad DFT arguments");
+    DftPlane p;
+    p.comp = comp;
+    p.z = z_plane;
+    p.first = first_step;
+    p.interval = sample_interval;
+    p.nfreq = nfreq;
+    p.cast_f32 = cast_f32 ? 1 : 0;
+    p.freq.assign(freq_hz, freq_hz + nfreq);
+    int rc = dalloc(ctx, (void**)&p.acc, (size_t)nfreq * ctx->nx * ctx->ny * 2 * sizeof(double));
+    if (rc) return rc;
+    ctx->dft.push_back(p);
+    rc = relayout_step_inputs(ctx);
+    if (rc) return rc;
+    drop_graphs(ctx);
+    *id = (int32_t)ctx->dft.size() - 1;
+    return PHP_OK;
+}
+
+int php_dft_read(php_ctx* ctx, int32_t id, double* out, int32_t* nsamples)
+{
+    if (!ctx || !out) return PHP_ERR_INPUT;
+    if (id < 0 || id >= (int)ctx->dft.size()) return fail(ctx, PHP_ERR_INPUT, "no DFT plane %d", id);
+    const DftPlane& p = ctx->dft[id];
+    CK(cudaMemcpyAsync(out, p.acc, (size_t)p.nfreq * ctx->nx * ctx->ny * 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (nsamples) *nsamples = p.nsamples;
+    return PHP_OK;
+}
+
+int php_memory_bytes(const php_ctx* ctx, uint64_t* bytes)
+{
+    if (!ctx || !bytes) return PHP_ERR_INPUT;
+    *bytes = ctx->bytes;
+    return PHP_OK;
+}
+
+int php_last_launch_count(const php_ctx* ctx, int32_t* launches)
+{
+    if (!ctx || !launches) return PHP_ERR_INPUT;
+    *launches = ctx->last_launches;
+    return PHP_OK;
+}
+
+int php_stream(const php_ctx* ctx, void** stream)
+{
+    if (!ctx || !stream) return PHP_ERR_INPUT;
+    *stream = (void*)ctx->stream;
+    return PHP_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,280 @@
+/*
+ * fdtd_b200 -- drop-in replacement for PhP_FDTD's solver executable
+ * (fdtd.x, fdtd.c:2075-4083) on one B200.
+ *
+ *   fdtd_b200 <config.cfg> [fp64|fp64-strict|fp32]
+ *
+ * Reads the same .cfg, medium_map.bin and material files, prints the same
+ * progress lines and writes the same output files as a single-rank run of
+ * the reference:
+ *   field_slice_<axis><pos>_<step:08d>.bin   every output_interval steps
+ *   monitor_point.dat (monitor_output_file)  every step
+ *   full_monitor.dat                         every output_interval steps
+ *   source.txt                               every output_interval steps
+ * The time loop (fdtd.c:3116-3884) runs on the GPU through libphpfdtd; this
+ * file is the host loop around it, with the reference's output cadence and
+ * index conventions (monitor and z-slice fields read at k+1, atoms at k,
+ * fdtd.c:1029, 3752-3753, 3814-3815).
+ *
+ * Exit codes: 0 done, 1 usage / divergence abort (as MPI_Abort(1) at
+ * fdtd.c:3667), 2 bad input, 3 device failure.
+ */
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+#include "php_fdtd.h"
+#include "php_host.h"
+
+static double wall(void)
+{
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
+static int device_fail(php_ctx* ctx, const char* what, int rc)
+{
+    fprintf(stderr, "%s failed (%d): %s\n", what, rc, php_last_error(ctx));
+    return rc == PHP_ERR_INPUT ? 2 : 3;
+}
+
+static void print_config(const php_cfg* c)
+{
+    printf("==========================Simulation Configuration===========================\n");
+    printf("  Grid size: %d x %d x %d\n", c->nx, c->ny, c->nz);
+    printf("  Spatial steps: dx=%.4e m, dy=%.4e m, dz=%.4e m\n", c->delta_x, c->delta_y, c->delta_z);
+    printf("  Time steps: %d, dt=%.4e s\n", c->tsteps, c->dt);
+    printf("  PML thickness: %d cells\n", c->pml_thickness);
+    printf("  PML reflection: %.4g\n", c->pml_reflection);
+    printf("  Medium file: %s\n", c->medium_file);
+    printf("  Sources: %d\n", c->num_sources);
+    for (int i = 0; i < c->num_sources; i++) {
+        const php_source_desc* s = &c->sources[i];
+        const char* ts = s->type == 1 ? "sinusoidal" : s->type == 2 ? "ricker" : s->type == 3 ? "dipole" : "gaussian";
+        printf("    Source %d: type=%s, position=(%d,%d,%d), amplitude=%.2f\n", i + 1, ts, s->x, s->y, s->z, s->amplitude);
+        printf("               component=%c, frequency=%.2e Hz, T=%.2e s, t0=%.2e s, tau=%.2e s\n", (char)s->component,
+               s->frequency, 1 / s->frequency, s->t0, s->tau);
+    }
+    printf("Output %.2s at time interval: %.2e s\n", c->output_component, c->output_interval * c->dt);
+    printf("Output slice: axis=%c, position=%d\n", c->output_slice_axis, c->output_slice_position);
+    printf("\nMaterial library details:\n");
+    for (int i = 0; i < c->num_materials; i++) {
+        const php_host_material* m = &c->materials[i];
+        printf("  Material %d: %s\n", i, m->name);
+        printf("    Dielectric tensor (real):\n");
+        for (int r = 0; r < 3; r++) printf("      [%.4f, %.4f, %.4f]\n", m->eps_re[3 * r], m->eps_re[3 * r + 1], m->eps_re[3 * r + 2]);
+        printf("    Dielectric tensor (imag) should be >= 0:\n");
+        for (int r = 0; r < 3; r++) printf("      [%.4f, %.4f, %.4f]\n", m->eps_im[3 * r], m->eps_im[3 * r + 1], m->eps_im[3 * r + 2]);
+        printf("    use_ADE: %d\n    Number of atoms: %d\n", m->use_ade, m->natom);
+    }
+}
+
+static void write_monitor_row(const php_cfg* cfg, FILE** f, int with_rv, int natom, int step, const double* row)
+{
+    if (step == 0) {
+        *f = fopen(cfg->monitor_output_file, "w");
+        if (*f) php_monitor_header(*f, with_rv);
+    }
+    if (!*f) return;
+    const int idx = cfg->monitor_atom * 3 + cfg->monitor_dir;
+    const double r = with_rv ? row[9 + idx] : 0.0, v = with_rv ? row[9 + 3 * natom + idx] : 0.0;
+    php_monitor_row(*f, step * cfg->dt, row, with_rv, r, v);
+}
+
+int main(int argc, char** argv)
+{
+    printf("FDTD (B200) running on 1 GPU\n");
+    if (argc < 2) {
+        printf("Usage: %s <config_file.cfg> [fp64|fp64-strict|fp32]\n", argv[0]);
+        return 1;
+    }
+    int precision = PHP_PREC_FP64;
+    const char* pa = argc > 2 ? argv[2] : getenv("PHP_PRECISION");
+    if (pa) {
+        if (!strcmp(pa, "fp64-strict")) precision = PHP_PREC_FP64_STRICT;
+        else if (!strcmp(pa, "fp32")) precision = PHP_PREC_FP32;
+        else if (!strcmp(pa, "fp64")) precision = PHP_PREC_FP64;
+        else {
+            fprintf(stderr, "unknown precision '%s'\n", pa);
+            return 1;
+        }
+    }
+    char err[1024] = "";
+    php_cfg* cfg = NULL;
+    if (php_cfg_load(argv[1], &cfg, err, sizeof(err))) {
+        fprintf(stderr, "%s\n", err);
+        return 2;
+    }
+    if (cfg->warnings[0]) fprintf(stderr, "%s", cfg->warnings);
+    print_config(cfg);
+    printf("Using medium file: %s\n", cfg->medium_file);
+    int32_t* medium = NULL;
+    if (php_medium_load(cfg->medium_file, cfg->nx, cfg->ny, cfg->nz, &medium, err, sizeof(err))) {
+        fprintf(stderr, "%s\n", err);
+        php_cfg_free(cfg);
+        return 2;
+    }
+    printf("Successfully loaded medium map from %s\n", cfg->medium_file);
+
+    php_desc desc;
+    php_cfg_to_desc(cfg, medium, precision, &desc);
+    php_ctx* ctx = NULL;
+    int rc = php_create(&desc, &ctx);
+    if (rc) {
+        int code = device_fail(NULL, "php_create", rc);
+        free(medium);
+        php_cfg_free(cfg);
+        return code;
+    }
+
+    const int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz;
+    /* monitor point: fields at z+1, atoms at z (fdtd.c:3806-3883) */
+    int monitor_ok = 0, monitor_rv = 0, monitor_natom = 0;
+    if (cfg->monitor_enabled && cfg->monitor_z >= 0 && cfg->monitor_z < nz && cfg->monitor_x >= 0 && cfg->monitor_x < nx &&
+        cfg->monitor_y >= 0 && cfg->monitor_y < ny) {
+        monitor_ok = 1;
+        int id = medium[((size_t)cfg->monitor_x * ny + cfg->monitor_y) * nz + cfg->monitor_z];
+        monitor_natom = cfg->materials[id].natom;
+        monitor_rv = cfg->monitor_atom < monitor_natom;
+        /* fdtd.c:2932-2951: atoms at the monitor point switch the full monitor on */
+        if (!cfg->full_monitor_enabled && monitor_natom > 0) cfg->full_monitor_enabled = 1;
+        if ((rc = php_probe_set(ctx, cfg->monitor_x, cfg->monitor_y, cfg->monitor_z + 1, cfg->monitor_z)))
+            return device_fail(ctx, "php_probe_set", rc);
+    }
+    int full_ok = 0, full_natom = 0;
+    if (cfg->full_monitor_enabled && cfg->monitor_z >= 0 && cfg->monitor_z < nz && cfg->monitor_x >= 0 && cfg->monitor_x < nx &&
+        cfg->monitor_y >= 0 && cfg->monitor_y < ny) {
+        full_ok = 1;
+        full_natom = cfg->materials[medium[((size_t)cfg->monitor_x * ny + cfg->monitor_y) * nz + cfg->monitor_z]].natom;
+    }
+    free(medium);
+    medium = NULL;
+
+    FILE* source_file = fopen("source.txt", "w");
+    if (!source_file) fprintf(stderr, "Error opening source.txt for writing\n");
+    FILE* monitor_file = NULL;
+    FILE* full_file = NULL;
+    const int comp = php_component_from_name(cfg->output_component);
+    const char axis = cfg->output_slice_axis;
+    const int spos = cfg->output_slice_position;
+    size_t slice_n = axis == 'z' ? (size_t)nx * ny : axis == 'x' ? (size_t)ny * nz : (size_t)nx * nz;
+    float* slice = (float*)malloc(slice_n * sizeof(float));
+    const int max_rows = cfg->output_interval + 1;
+    double* rows = (double*)malloc((size_t)max_rows * (9 + 6 * (monitor_natom > 0 ? monitor_natom : 1)) * sizeof(double));
+    double* rv = (double*)malloc(sizeof(double) * 6 * (full_natom > 0 ? full_natom : 1));
+
+    const double start = wall();
+    printf("Entering iteration:\n");
+    fflush(stdout);
+    int t = 0;
+    int exit_code = 0;
+    while (t < cfg->tsteps) {
+        /* run to the next output step (t % output_interval == 0) inclusive */
+        int next = (t % cfg->output_interval == 0) ? t : (t / cfg->output_interval + 1) * cfg->output_interval;
+        if (next > cfg->tsteps - 1) next = cfg->tsteps - 1;
+        const int n = next - t + 1;
+        if ((rc = php_step(ctx, n))) { exit_code = device_fail(ctx, "php_step", rc); break; }
+        /* source.txt rows of the output steps in this chunk (fdtd.c:3359-3400) */
+        for (int s = t; s <= next; s++) {
+            if (s % cfg->output_interval == 0 && source_file) {
+                double ct = s * cfg->dt;
+                fprintf(source_file, "%.4e  ", ct);
+                for (int q = 0; q < cfg->num_sources; q++) fprintf(source_file, "%.4e  ", php_source_value(&cfg->sources[q], ct));
+                fprintf(source_file, "\n");
+                fflush(source_file);
+            }
+        }
+        /* monitor rows (every step, fdtd.c:3806-3883): the row of an output
+         * step follows that step's diagnostics, so a divergence abort there
+         * drops it, as in the reference */
+        int nrows = 0, row_len = 0;
+        if (monitor_ok) {
+            if ((rc = php_probe_read(ctx, rows, max_rows, &nrows, &row_len))) { exit_code = device_fail(ctx, "php_probe_read", rc); break; }
+            for (int q = 0; q < nrows && t + q < next; q++) write_monitor_row(cfg, &monitor_file, monitor_rv, monitor_natom, t + q, rows + (size_t)q * row_len);
+        }
+        const int last = next;
+        if (last % cfg->output_interval == 0) {
+            php_diag dg;
+            if ((rc = php_diagnostics(ctx, &dg))) { exit_code = device_fail(ctx, "php_diagnostics", rc); break; }
+            double current_time = last * cfg->dt;
+            printf("it %d/%d (%.1f%%), t = %.5e s,|E|_max = %.2e V/m,", last, cfg->tsteps, 100.0 * last / cfg->tsteps, current_time,
+                   dg.max_e);
+            printf("r_max = %.2e A,", dg.max_r / 1e-10);
+            if (last > 0) {
+                double el = wall() - start;
+                double eta = el / last * (cfg->tsteps - last);
+                int eh = (int)(el / 3600), em = (int)((el - eh * 3600) / 60), es = (int)(el - eh * 3600 - em * 60);
+                int rh = (int)(eta / 3600), rm = (int)((eta - rh * 3600) / 60), rs = (int)(eta - rh * 3600 - rm * 60);
+                printf(" elapsed: %03d:%02d:%02d, ETA: %03d:%02d:%02d", eh, em, es, rh, rm, rs);
+            }
+            printf("\n");
+            fflush(stdout);
+            if (dg.max_r > 1e-10) { /* fdtd.c:3626-3668 */
+                const int* am = dg.argmax_r;
+                printf("ERROR: r field too large at step %d\n", last);
+                printf("Max r value: %e\n", dg.max_r);
+                printf("Location: i=%d, j=%d, k=%d (global k=%d)\n", am[0], am[1], am[2], am[2]);
+                printf("Atom: %d, Direction: %d\n", am[3], am[4]);
+                int na = 0;
+                double rr[192], vv[192], e9[9];
+                php_read_cell_state(ctx, am[0], am[1], am[2], &na, rr, vv, NULL, NULL);
+                php_read_point(ctx, am[0], am[1], am[2], e9);
+                int idx = am[3] * 3 + am[4];
+                printf("v value: %e\n", vv[idx]);
+                /* acceleration recomputed from the lab-frame E, as fdtd.c:3642-3663 */
+                const php_host_material* m = NULL;
+                int32_t* med = NULL;
+                if (!php_medium_load(cfg->medium_file, nx, ny, nz, &med, err, sizeof(err))) {
+                    m = &cfg->materials[med[((size_t)am[0] * ny + am[1]) * nz + am[2]]];
+                    free(med);
+                }
+                if (m && m->qezm && m->dmm) {
+                    double a_val = 0.0;
+                    for (int iE = 0; iE < 3; iE++) a_val += m->qezm[am[3] * 9 + iE * 3 + am[4]] * e9[iE];
+                    for (int q = 0; q < 3 * m->natom; q++) a_val -= m->dmm[(size_t)idx * 3 * m->natom + q] * rr[q];
+                    printf("a value: %e\n", a_val);
+                }
+                fflush(stdout);
+                exit_code = 1;
+                break;
+            }
+            char name[256];
+            php_slice_filename(name, sizeof(name), axis, spos, last);
+            if (php_read_slice(ctx, comp, axis, spos, slice) == PHP_OK) php_write_slice_file(name, axis, nx, ny, nz, slice);
+            else fprintf(stderr, "%s\n", php_last_error(ctx));
+            if (full_ok) {
+                double e9[9];
+                int na = 0;
+                php_read_point(ctx, cfg->monitor_x, cfg->monitor_y, cfg->monitor_z + 1, e9);
+                php_read_cell_state(ctx, cfg->monitor_x, cfg->monitor_y, cfg->monitor_z, &na, rv, rv + 3 * full_natom, NULL, NULL);
+                if (last == 0) {
+                    full_file = fopen(cfg->full_monitor_output_file, "w");
+                    if (full_file) php_full_monitor_header(full_file, full_natom);
+                }
+                if (full_file) php_full_monitor_row(full_file, current_time, e9, full_natom, rv, rv + 3 * full_natom);
+            }
+        }
+        if (monitor_ok && nrows == n) write_monitor_row(cfg, &monitor_file, monitor_rv, monitor_natom, next, rows + (size_t)(n - 1) * row_len);
+        t = next + 1;
+    }
+    php_sync(ctx);
+    if (source_file) fclose(source_file);
+    if (monitor_file) {
+        fclose(monitor_file);
+        printf("Monitor data saved to %s\n", cfg->monitor_output_file);
+    }
+    if (full_file) {
+        fclose(full_file);
+        printf("Full monitor data saved to %s\n", cfg->full_monitor_output_file);
+    }
+    if (exit_code == 0) printf("\nSimulation completed in %.2f seconds\n", wall() - start);
+    free(slice);
+    free(rows);
+    free(rv);
+    php_destroy(ctx);
+    php_cfg_free(cfg);
+    return exit_code;
+}
