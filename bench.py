@@ -1,0 +1,461 @@
+"""Benchmark of the PhP_FDTD time-step loop on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload cfg1] [--precision fp64|fp32|fp64-strict]
+
+One step = one FDTD time step (H sweep, fused D/source/E/ADE/ion sweep,
+monitor probe, running DFT) over the whole domain of the workload.  The
+default workload is the 256^3 tensor-ADE configuration (Drude-Lorentz tip
+over a rotated lossy anisotropic slab, 12-cell CPML, sine source at
+900 cm^-1, running DFT 2 cells above the slab), synthetic inputs from a
+fixed seed.  The field state (9 x 16.8 M cells, 1.2 GB in FP64) is far larger
+than L2, so no flush is needed between steps.
+
+Prints one JSON line on rank 0.  With --gpus N (torchrun) every rank advances
+its own replica of the domain (weak scaling, no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {"cfg0": 0, "cfg1": 1, "cfg2": 2, "cfg4": 4}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=400)
+    p.add_argument("--warmup", type=int, default=20)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="cfg1", choices=sorted(WORKLOADS))
+    p.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "fp64-strict"])
+    p.add_argument("--scale", type=float, default=1.0, help="grid scale (1.0 = the configuration's grid)")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--case-dir", default=None)
+    return p.parse_args()
+
+
+# ----------------------------------------------------------------- plumbing
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append({"sm": float(f[1]), "max": float(f[2]), "power": float(f[3]), "hw": f[5], "hwt": f[6],
+                             "swt": f[7], "swp": f[8]})
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        reasons = set()
+        for r in rows:
+            for key, name in (("hw", "hw_slowdown"), ("hwt", "hw_thermal_slowdown"), ("swt", "sw_thermal_slowdown"),
+                              ("swp", "sw_power_cap")):
+                if r[key].lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(r["sm"] for r in rows), "sm_max_mhz": max(r["max"] for r in rows),
+                "power_w_max": max(r["power"] for r in rows), "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# ------------------------------------------------------------------ workload
+
+
+def make_case(workload: str, scale: float, tsteps: int, case_dir: Path) -> Path:
+    from php_fdtd_b200.workloads import baseline_case, write_case
+    spec = baseline_case(WORKLOADS[workload], tsteps=tsteps, scale=scale)
+    cfg = case_dir / "case.cfg"
+    stamp = case_dir / "stamp.json"
+    key = {"workload": workload, "scale": scale, "tsteps": tsteps}
+    if cfg.exists() and stamp.exists() and json.loads(stamp.read_text()) == key:
+        return cfg
+    write_case(spec, case_dir)
+    stamp.write_text(json.dumps(key))
+    return cfg
+
+
+def census(cfg, medium: np.ndarray):
+    """Cell counts per material class and PML membership (algorithmic bytes)."""
+    nx, ny, nz, L = cfg.nx, cfg.ny, cfg.nz, cfg.pml_thickness
+    mats = cfg.materials
+    ade = np.array([m.use_ade == 1 for m in mats])
+    lossy = np.array([(m.use_ade == 0) and any(m.eps_im[q] != 0 for q in range(9)) for m in mats])
+    natom = np.array([m.natom for m in mats])
+    ids, counts = np.unique(medium, return_counts=True)
+    c = dict(zip(ids.tolist(), counts.tolist()))
+    n_ade = sum(v for k, v in c.items() if ade[k])
+    n_lossy = sum(v for k, v in c.items() if lossy[k])
+    atom_words = sum(v * 12 * natom[k] for k, v in c.items())
+    n_atom_cells = sum(v for k, v in c.items() if natom[k] > 0)
+
+    def pml_count(n):
+        idx = np.arange(n)
+        return int(np.sum((idx < L) | (idx >= n - L))) if L > 0 else 0
+    px, py, pz = pml_count(nx), pml_count(ny), pml_count(nz)
+    # PML axis memberships summed over cells (H sweep covers i<nx-1, j<ny-1)
+    pml_e = px * ny * nz + nx * py * nz + nx * ny * pz
+    pml_h = (min(px, nx - 1) * (ny - 1) * nz + (nx - 1) * min(py, ny - 1) * nz + (nx - 1) * (ny - 1) * pz)
+    return {"cells": nx * ny * nz, "h_cells": (nx - 1) * (ny - 1) * nz, "ade_cells": n_ade, "lossy_cells": n_lossy,
+            "atom_cells": n_atom_cells, "atom_words": int(atom_words), "pml_e": pml_e, "pml_h": pml_h}
+
+
+def algorithmic_bytes(c: dict, s: int):
+    """Compulsory state traffic per launch: H sweep reads E, H and writes H
+    (9 words), plus 4 psi words per PML axis; the fused sweep reads H, D and
+    writes D, E (12 words), plus old E in lossy/ADE cells (3), P and P_old
+    (12) in ADE cells, r and v (12 N) in atom cells, 4 psi words per PML
+    axis, and the 1-byte material id."""
+    h = s * (9 * c["h_cells"] + 4 * c["pml_h"])
+    e = s * (12 * c["cells"] + 3 * (c["ade_cells"] + c["lossy_cells"]) + 12 * c["ade_cells"] + c["atom_words"]
+             + 4 * c["pml_e"]) + c["cells"]
+    return h, e
+
+
+# ------------------------------------------------------------------ our arm
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    from php_fdtd_b200 import Config, Simulation
+
+    case_dir = Path(args.case_dir or tempfile.gettempdir()) / f"php_bench_{args.workload}_{args.scale}_r{rank}"
+    case_dir.mkdir(parents=True, exist_ok=True)
+    tsteps = args.warmup + 3 * args.steps + 8
+    cfg_path = make_case(args.workload, args.scale, tsteps, case_dir)
+    old = os.getcwd()
+    os.chdir(case_dir)
+    try:
+        cfg = Config.load("case.cfg")
+        medium = cfg.load_medium()
+    finally:
+        os.chdir(old)
+    holder = cfg.desc(medium, args.precision)
+    holder.desc.device = local
+    sim = Simulation(holder)
+    nx, ny, nz = cfg.nx, cfg.ny, cfg.nz
+    V = nx * ny * nz
+    oi = cfg.output_interval
+    # per-step extras of the configuration: monitor probe and running DFT
+    sim.probe_set(cfg.monitor_x, cfg.monitor_y, cfg.monitor_z + 1, cfg.monitor_z)
+    dft_plane = cfg.output_slice_position + 1
+    f_src = cfg.unique_source_frequency
+    sim.dft_add("Ez", dft_plane, [f_src], first_step=0, interval=1)
+    stream = torch.cuda.ExternalStream(sim.stream, device=torch.device("cuda", local))
+
+    # warm-up (records the step graphs)
+    sim.step(args.warmup)
+    sim.probe_read()
+    sim.sync()
+
+    # ---- device-resident timed region
+    barrier(ws)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        ev0.record(stream)
+        remaining = args.steps
+        while remaining > 0:  # the probe ring holds 8192 rows; drain between blocks
+            n = min(remaining, 4096)
+            sim.step(n)
+            remaining -= n
+            if remaining > 0:
+                sim.probe_read()
+        ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    barrier(ws)
+    ms = ev0.elapsed_time(ev1)
+    launches_per_step = 2 + 1 + 1
+    sim.probe_read()
+    ms_max = max_over_ranks(ms, ws)
+    value = V * args.steps * ws / (ms_max * 1e-3) / 1e9
+
+    # ---- per-kernel device time (event nodes inside the step graphs)
+    sim.profile(True)
+    sim.step(min(args.steps, 200))
+    prof = sim.profile_read()
+    sim.profile(False)
+    sim.probe_read()
+
+    # ---- end to end through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        slice_buf_bytes = 4 * (nx * ny if cfg.output_slice_axis == "z" else (ny * nz if cfg.output_slice_axis == "x" else nx * nz))
+        row_len = 9 + 6 * 0
+        sim.sync()
+        barrier(ws)
+        t0 = time.perf_counter()
+        done = 0
+        d2h = 0
+        h2d = 0
+        while done < args.steps:
+            n = min(oi, args.steps - done)
+            sim.step(n)                       # per-step source values and DFT phasors copied host -> device
+            h2d += n * 8 * (cfg.num_sources + 3)
+            rows = sim.probe_read()           # monitor rows, device -> host
+            d2h += rows.nbytes
+            sim.diagnostics()                 # |E|max, r max, device -> host
+            d2h += 32
+            sim.read_slice("Ez", cfg.output_slice_axis, cfg.output_slice_position)
+            d2h += slice_buf_bytes
+            done += n
+        sim.sync()
+        t1 = time.perf_counter()
+        barrier(ws)
+        e2e_s = max_over_ranks(t1 - t0, ws)
+        e2e = {"value": round(V * args.steps * ws / e2e_s / 1e9, 4), "unit": "Gcell-updates/s",
+               "h2d_bytes_per_step": round(h2d / args.steps, 1), "d2h_bytes_per_step": round(d2h / args.steps, 1),
+               "path": "php_step/php_probe_read/php_diagnostics/php_read_slice per output interval "
+                       f"({oi} steps), host buffers"}
+
+    s = 4 if args.precision == "fp32" else 8
+    c = census(cfg, medium)
+    hb, eb = algorithmic_bytes(c, s)
+    peaks = {}
+    pk = ROOT / "MEASURED_PEAKS.json"
+    if pk.exists():
+        peaks = json.loads(pk.read_text())
+    peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    e_ms = prof["e_sweep"]["ms"] / max(1, prof["e_sweep"]["launches"])
+    h_ms = prof["h_sweep"]["ms"] / max(1, prof["h_sweep"]["launches"])
+    e_gbs = eb / (e_ms * 1e-3) / 1e9
+    h_gbs = hb / (h_ms * 1e-3) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / f"traffic_{args.workload}_{args.precision}.json"
+    if tf.exists() and args.scale == 1.0:
+        traffic = json.loads(tf.read_text()).get("e_sweep_dram_bytes_per_launch")
+    return sim, cfg, {
+        "value": value, "ms": ms_max, "V": V, "clocks": clocks.summary(), "prof": prof, "e2e": e2e,
+        "launches_per_step": launches_per_step, "census": c, "roofline": {
+            "bound": "hbm", "kernel": "e_sweep (fused D/source/E/ADE/ion sweep)",
+            "achieved": round(e_gbs, 1), "peak": peak, "unit": "GB/s", "frac": round(e_gbs / peak, 4),
+            "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured" else "fallback 6650",
+            "traffic": traffic, "algorithmic_bytes_per_launch": eb, "avg_launch_ms": round(e_ms, 5),
+            "h_sweep": {"achieved": round(h_gbs, 1), "frac": round(h_gbs / peak, 4), "avg_launch_ms": round(h_ms, 5),
+                        "algorithmic_bytes_per_launch": hb},
+            "kernel_share": {k: round(v["ms"] / max(1e-9, sum(x["ms"] for x in prof.values())), 4) for k, v in prof.items()}}}
+
+
+# ------------------------------------------------------ reference / baseline
+
+
+def reference_rate(case_cfg: Path, steps: int, timeout: int = 900):
+    """Runs the reference solver (compiled from its own sources, single
+    rank) on the workload for `steps` time steps; its own loop timer
+    (fdtd.c:3110, 3915) gives the throughput."""
+    from oracle import reference_binary
+    exe = reference_binary("fast")
+    if not exe.exists():
+        exe = reference_binary("plain")
+    if not exe.exists():
+        return None, "reference binary not built (make -C oracle ref)"
+    case_dir = case_cfg.parent
+    text = case_cfg.read_text()
+    text = re.sub(r"(?m)^tsteps = \d+", f"tsteps = {steps}", text)
+    text = re.sub(r"(?m)^output_interval = \d+", f"output_interval = {max(1, steps)}", text)
+    run_dir = case_dir / "refrun"
+    run_dir.mkdir(exist_ok=True)
+    for p in case_dir.iterdir():
+        if p.is_file() and p.name not in ("case.cfg",):
+            dst = run_dir / p.name
+            if not dst.exists():
+                os.symlink(p, dst)
+    (run_dir / "case.cfg").write_text(text)
+    t0 = time.perf_counter()
+    pr = subprocess.run([str(exe), "case.cfg"], cwd=run_dir, capture_output=True, text=True, timeout=timeout)
+    wall = time.perf_counter() - t0
+    m = re.search(r"Simulation completed in ([\d.]+) seconds", pr.stdout)
+    if pr.returncode != 0 or not m:
+        return None, f"reference run failed rc={pr.returncode}: {pr.stdout[-300:]} {pr.stderr[-300:]}"
+    return {"loop_s": float(m.group(1)), "wall_s": wall, "steps": steps, "exe": exe.name}, None
+
+
+def cpu_model():
+    try:
+        for l in open("/proc/cpuinfo"):
+            if l.startswith("model name"):
+                return l.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def ref_sample_steps(V: int, k: int) -> int:
+    # about 2e8 cell updates (~10-30 s on one core of the reference)
+    return int(max(2, min(k, round(2e8 / V))))
+
+
+def run_reference_arm(args, ws, rank):
+    if rank != 0:
+        return
+    case_dir = Path(args.case_dir or tempfile.gettempdir()) / f"php_bench_{args.workload}_{args.scale}_ref"
+    case_dir.mkdir(parents=True, exist_ok=True)
+    cfg_path = make_case(args.workload, args.scale, 10, case_dir)
+    from php_fdtd_b200.workloads import baseline_case
+    spec = baseline_case(WORKLOADS[args.workload], scale=args.scale)
+    V = spec.nx * spec.ny * spec.nz
+    steps = ref_sample_steps(V, args.steps)
+    # warm-up sample (page cache, allocator) then the timed sample
+    if args.warmup > 0:
+        reference_rate(cfg_path, 1)
+    res, err = reference_rate(cfg_path, steps)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": err}))
+        return
+    rate = V * steps / res["loop_s"] / 1e9
+    line = {
+        "metric": metric_name(args), "value": round(rate, 6), "unit": "Gcell-updates/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(res["loop_s"] / steps * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": workload_name(args), "grid": [spec.nx, spec.ny, spec.nz], "cells": V},
+        "cpu_baseline": {"value": round(rate, 6), "unit": "Gcell-updates/s", "cores": 1, "kind": "reference",
+                         "sample": f"{steps} time steps of the full {spec.nx}x{spec.ny}x{spec.nz} domain, reference "
+                                   f"solver ({res['exe']}, -Ofast, one MPI rank through the single-rank MPI stub), "
+                                   f"timed by its own loop timer; CPU {cpu_model()}"},
+        "e2e": {"value": round(rate, 6), "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def metric_name(args):
+    return f"Gcell-updates/s, {args.precision.upper()} path"
+
+
+def workload_name(args):
+    from php_fdtd_b200.workloads import BASELINE_NAMES
+    return BASELINE_NAMES[WORKLOADS[args.workload]] + ("" if args.scale == 1.0 else f" (scale {args.scale})")
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_init()
+    if args.impl == "reference":
+        run_reference_arm(args, ws, rank)
+        barrier(ws)
+        return
+    sim, cfg, r = run_ours(args, ws, rank, local)
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline and ws == 1:
+            case_dir = Path(args.case_dir or tempfile.gettempdir()) / f"php_bench_{args.workload}_{args.scale}_r{rank}"
+            steps = ref_sample_steps(r["V"], args.steps)
+            res, err = reference_rate(case_dir / "case.cfg", steps)
+            if res:
+                cpu = {"value": round(r["V"] * steps / res["loop_s"] / 1e9, 6), "unit": "Gcell-updates/s", "cores": 1,
+                       "kind": "reference",
+                       "sample": f"{steps} time steps of the full domain, reference solver {res['exe']} (one MPI rank "
+                                 f"through the single-rank stub, its own loop timer); CPU {cpu_model()}"}
+            else:
+                cpu = {"value": None, "unit": "Gcell-updates/s", "cores": 1, "kind": "reference", "sample": err}
+        line = {
+            "metric": metric_name(args), "value": round(r["value"], 4), "unit": "Gcell-updates/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(r["ms"] / args.steps, 5),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": {"fp64": "f64", "fp32": "f32", "fp64-strict": "f64"}[args.precision], "data": "synthetic",
+            "config": {"workload": workload_name(args), "grid": [cfg.nx, cfg.ny, cfg.nz], "cells": r["V"],
+                       "precision": args.precision, "parallelism": f"replicas x{ws}" if ws > 1 else "single domain",
+                       "l2": "state 9 fields x cells > L2 (126 MB); no flush needed",
+                       "per_step": "H sweep + fused D/source/E/ADE sweep + monitor probe + running DFT (1 plane)"},
+            "hbm_gbs": r["roofline"]["achieved"],
+            "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": r["e2e"], "clocks": r["clocks"],
+            "gpu_launches": r["launches_per_step"] * args.steps,
+            "kernel_profile": r["prof"],
+        }
+        print(json.dumps(line))
+    sim.close()
+    barrier(ws)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -222,6 +222,14 @@ int php_last_launch_count(const php_ctx* ctx, int32_t* launches);
 /* Stream the context enqueues on (a cudaStream_t), for event timing. */
 int php_stream(const php_ctx* ctx, void** stream);
 
+/* Per-kernel timing.  While enabled, the recorded step graphs carry CUDA
+ * events around every sweep kernel and php_step accumulates their device
+ * time: ms[0] H sweep, ms[1] fused D/E sweep, ms[2] probe, ms[3] DFT, with
+ * the number of launches of each in launches[0..3].  Enabling or disabling
+ * resets the sums. */
+int php_profile_enable(php_ctx* ctx, int32_t enable);
+int php_profile_read(php_ctx* ctx, double* ms4, int64_t* launches4);
+
 #ifdef __cplusplus
 }
 #endif

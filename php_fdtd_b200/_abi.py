@@ -96,6 +96,8 @@ DEVICE_SYMBOLS = {
     "php_memory_bytes": (_i, [C.c_void_p, C.POINTER(C.c_uint64)]),
     "php_last_launch_count": (_i, [C.c_void_p, C.POINTER(_i)]),
     "php_stream": (_i, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "php_profile_enable": (_i, [C.c_void_p, _i]),
+    "php_profile_read": (_i, [C.c_void_p, _dp, C.POINTER(C.c_int64)]),
 }
 
 HOST_SYMBOLS = {

@@ -103,6 +103,12 @@ struct php_ctx {
     int32_t* probe_count = nullptr;
 
     std::vector<DftPlane> dft;
+
+    /* per-kernel timing (php_profile_enable) */
+    bool profile = false;
+    std::vector<cudaEvent_t> prof_ev;   /* [kMaxChunk][4 kinds][begin, end] */
+    double prof_ms[4] = {};
+    int64_t prof_n[4] = {};
 };
 
 /* ------------------------------------------------------------------ utils */
@@ -446,24 +452,37 @@ static StepArgs<R> make_args(php_ctx* ctx, int s_local)
     return a;
 }
 
+static inline void prof_mark(php_ctx* ctx, int s_local, int kind, int end)
+{
+    if (ctx->profile)
+        cudaEventRecordWithFlags(ctx->prof_ev[((size_t)s_local * 4 + kind) * 2 + end], ctx->stream, cudaEventRecordExternal);
+}
+
 template <typename R, bool STRICT, int NA>
 static void launch_step_t(php_ctx* ctx, int s_local, int& launches)
 {
     StepArgs<R> a = make_args<R>(ctx, s_local);
     dim3 block(kBlockX, 8, 1);
     dim3 grid((ctx->nx + kBlockX - 1) / kBlockX, (ctx->ny + 7) / 8, (ctx->nz + ctx->zchunk - 1) / ctx->zchunk);
+    prof_mark(ctx, s_local, 0, 0);
     h_sweep<R, STRICT><<<grid, block, 0, ctx->stream>>>(a);
+    prof_mark(ctx, s_local, 0, 1);
+    prof_mark(ctx, s_local, 1, 0);
     e_sweep<R, STRICT, NA><<<grid, block, 0, ctx->stream>>>(a);
+    prof_mark(ctx, s_local, 1, 1);
     launches += 2;
     if (ctx->probe) {
+        prof_mark(ctx, s_local, 2, 0);
         R* const* fp = reinterpret_cast<R* const*>(ctx->f);
         Fields<R> f{fp[0], fp[1], fp[2], fp[3], fp[4], fp[5], fp[6], fp[7], fp[8]};
         const int threads = (9 + 2 * ctx->probe_n3 + 31) / 32 * 32;
         probe_record_counted<R><<<1, threads, 0, ctx->stream>>>(
             f, ctx->probe_cf, (const R*)ctx->r, (const R*)ctx->v, ctx->nslot, ctx->probe_slot, ctx->probe_n3,
             ctx->probe_rows, ctx->probe_count, kProbeCap, 9 + 2 * ctx->probe_n3);
+        prof_mark(ctx, s_local, 2, 1);
         launches++;
     }
+    if (!ctx->dft.empty()) prof_mark(ctx, s_local, 3, 0);
     for (auto& p : ctx->dft) {
         R* const* fp = reinterpret_cast<R* const*>(ctx->f);
         const int64_t n = (int64_t)ctx->nx * ctx->ny;
@@ -473,6 +492,7 @@ static void launch_step_t(php_ctx* ctx, int s_local, int& launches)
                                                        p.in_off, p.in_off + 1, p.acc);
         launches++;
     }
+    if (!ctx->dft.empty()) prof_mark(ctx, s_local, 3, 1);
 }
 
 typedef void (*step_fn)(php_ctx*, int, int&);
@@ -541,6 +561,8 @@ static void ctx_free(php_ctx* ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (void* p : ctx->allocs) cudaFree(p);
     ctx->allocs.clear();
+    for (cudaEvent_t e : ctx->prof_ev) cudaEventDestroy(e);
+    ctx->prof_ev.clear();
     if (ctx->host_stage) cudaFreeHost(ctx->host_stage);
     if (ctx->step_in_host) cudaFreeHost(ctx->step_in_host);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -640,12 +662,18 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
         ctx->nsrc_active++;
     }
 
-    /* z chunking: enough blocks to cover 148 SMs several times over */
+    /* z chunking: short marches (8 planes measured best on 256^3, FP64 and
+     * FP32) while keeping at least ~4 waves of blocks on 148 SMs */
     {
-        const int tiles = ((nx + kBlockX - 1) / kBlockX) * ((ny + 7) / 8);
-        int nchunks = (int)std::max<int64_t>(1, std::min<int64_t>(nz, (2048 + tiles - 1) / tiles));
-        ctx->zchunk = d.z_chunk > 0 ? d.z_chunk : (nz + nchunks - 1) / nchunks;
+        const int tiles = ((nx + kBlockX - 1) / kBlockX) * ((ny + kBlockY - 1) / kBlockY);
+        int zc = std::min(8, nz);
+        while (zc > 1 && (int64_t)tiles * ((nz + zc - 1) / zc) < 148 * 4 * 4) zc /= 2;
+        ctx->zchunk = d.z_chunk > 0 ? d.z_chunk : zc;
     }
+    /* 32-bit cell offsets inside the sweeps */
+    if ((int64_t)ctx->plane * (nz + 2) >= ((int64_t)1 << 31))
+        return fail(ctx, PHP_ERR_UNSUPPORTED, "grid of %lld padded cells exceeds the 2^31 cell limit of one domain",
+                    (long long)ctx->plane * (nz + 2));
 
     /* allocations */
     const size_t rs = rsize(ctx->prec);
@@ -840,6 +868,17 @@ int php_step(php_ctx* ctx, int32_t nsteps)
         int rc = ensure_graph(ctx, n, &g);
         if (rc) return rc;
         CK(cudaGraphLaunch(g, ctx->stream));
+        if (ctx->profile) {
+            CK(cudaStreamSynchronize(ctx->stream));
+            for (int s = 0; s < n; s++)
+                for (int kind = 0; kind < 4; kind++) {
+                    if ((kind == 2 && !ctx->probe) || (kind == 3 && ctx->dft.empty())) continue;
+                    float ms = 0.f;
+                    CK(cudaEventElapsedTime(&ms, ctx->prof_ev[((size_t)s * 4 + kind) * 2], ctx->prof_ev[((size_t)s * 4 + kind) * 2 + 1]));
+                    ctx->prof_ms[kind] += ms;
+                    ctx->prof_n[kind] += kind == 3 ? (int64_t)ctx->dft.size() : 1;
+                }
+        }
         ctx->last_launches += n * (2 + (ctx->probe ? 1 : 0) + (int)ctx->dft.size());
         ctx->t += n;
         nsteps -= n;
@@ -1125,6 +1164,33 @@ int php_stream(const php_ctx* ctx, void** stream)
 {
     if (!ctx || !stream) return PHP_ERR_INPUT;
     *stream = (void*)ctx->stream;
+    return PHP_OK;
+}
+
+int php_profile_enable(php_ctx* ctx, int32_t enable)
+{
+    if (!ctx) return PHP_ERR_INPUT;
+    drop_graphs(ctx);
+    if (enable && ctx->prof_ev.empty()) {
+        ctx->prof_ev.resize((size_t)kMaxChunk * 4 * 2);
+        for (auto& e : ctx->prof_ev) CK(cudaEventCreate(&e));
+    }
+    ctx->profile = enable != 0;
+    for (int q = 0; q < 4; q++) {
+        ctx->prof_ms[q] = 0.0;
+        ctx->prof_n[q] = 0;
+    }
+    return PHP_OK;
+}
+
+int php_profile_read(php_ctx* ctx, double* ms4, int64_t* launches4)
+{
+    if (!ctx) return PHP_ERR_INPUT;
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int q = 0; q < 4; q++) {
+        if (ms4) ms4[q] = ctx->prof_ms[q];
+        if (launches4) launches4[q] = ctx->prof_n[q];
+    }
     return PHP_OK;
 }
 

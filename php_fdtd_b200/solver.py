@@ -271,7 +271,8 @@ class Simulation:
         return out
 
     def _slice_shape(self, axis: str):
-        return {"z": (self.nx, self.ny), "x": (self.ny, self.nz), "y": (self.nx, self.nz)}[axis]
+        # an unknown axis still goes to the library, which rejects it
+        return {"z": (self.nx, self.ny), "x": (self.ny, self.nz), "y": (self.nx, self.nz)}.get(axis, (1, 1))
 
     def read_slice(self, comp, axis: str, pos: int, f64: bool = False) -> np.ndarray:
         shape = self._slice_shape(axis)
@@ -345,6 +346,17 @@ class Simulation:
         v = C.c_int32()
         self._ck(self._lib.php_last_launch_count(self._ctx, C.byref(v)))
         return v.value
+
+    def profile(self, enable: bool = True):
+        """Per-kernel device timing of the following steps (php_profile_enable)."""
+        self._ck(self._lib.php_profile_enable(self._ctx, int(bool(enable))))
+
+    def profile_read(self) -> dict:
+        ms = np.zeros(4)
+        n = (C.c_int64 * 4)()
+        self._ck(self._lib.php_profile_read(self._ctx, ms.ctypes.data_as(C.POINTER(C.c_double)), n))
+        names = ("h_sweep", "e_sweep", "probe", "dft")
+        return {k: {"ms": float(ms[q]), "launches": int(n[q])} for q, k in enumerate(names)}
 
     @property
     def stream(self) -> int:
