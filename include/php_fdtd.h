@@ -230,6 +230,29 @@ int php_stream(const php_ctx* ctx, void** stream);
 int php_profile_enable(php_ctx* ctx, int32_t enable);
 int php_profile_read(php_ctx* ctx, double* ms4, int64_t* launches4);
 
+/* --- allocation-free field maxima ------------------------------------------ */
+
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory at the moment they need the field maxima: a divergence check on a
+ * device whose memory is full (a large domain takes most of the HBM, and a
+ * failing cudaMalloc would hide the real state), a host whose own allocator
+ * owns all device memory, or a latency-critical loop where cudaMalloc /
+ * cudaFree would synchronise the device.
+ *
+ * Computes, from three device arrays of n contiguous doubles, out2[0] =
+ * max sqrt(Ex^2+Ey^2+Ez^2) and out2[1] = max |Ex| (the values php_diagnostics
+ * reports as max_e and max_ex, fdtd.c:3537-3554) into out2, a device array
+ * of 2 doubles, asynchronously on `stream` (a cudaStream_t, NULL = legacy
+ * default stream).  It allocates nothing: its scratch is a fixed 256 KB
+ * array inside the library, which every GPU that loads the library holds
+ * until the process exits.  n above PHP_NOALLOC_MAX_CELLS is rejected with
+ * PHP_ERR_INPUT.  The first call on each device looks up the scratch
+ * address on that device (make it before any stream capture); calls that
+ * overlap on the GPU share the scratch and race, so serialise them. */
+#define PHP_NOALLOC_MAX_CELLS 67108864 /* 2^26 cells, e.g. 512 x 512 x 256 */
+int php_field_maxima_noalloc(const double* ex, const double* ey, const double* ez, int64_t n,
+                             double* out2, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -64,11 +64,11 @@ def build_host(verbose: bool = False) -> Path:
 
 def build_device(verbose: bool = False) -> Path:
     out = PKG / "libphpfdtd.so"
-    deps = [CSRC / "php_fdtd.cu", CSRC / "php_kernels.cuh", INC / "php_fdtd.h"]
-    deps += [p for p in CSRC.glob("*.cuh")]
+    sources = [CSRC / "php_fdtd.cu", CSRC / "php_noalloc.cu"]
+    deps = sources + [INC / "php_fdtd.h"] + [p for p in CSRC.glob("*.cuh")]
     if _stale(out, deps):
         _run([_nvcc(), *NVCC_ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",
-              "-shared", f"-I{INC}", CSRC / "php_fdtd.cu", "-o", out], verbose)
+              "-shared", f"-I{INC}", *sources, "-o", out], verbose)
     return out
 
 
