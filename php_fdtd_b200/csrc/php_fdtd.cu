@@ -14,6 +14,7 @@
 #include "php_kernels.cuh"
 
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
@@ -103,6 +104,11 @@ struct php_ctx {
     int32_t* probe_count = nullptr;
 
     std::vector<DftPlane> dft;
+
+    /* sweep kernels: TMA plane pipeline (default) or register prefetch */
+    bool use_tma = true;
+    TmaMaps maps;
+    int32_t* err_flag = nullptr;
 
     /* per-kernel timing (php_profile_enable) */
     bool profile = false;
@@ -449,6 +455,7 @@ static StepArgs<R> make_args(php_ctx* ctx, int s_local)
         a.src_comp[s] = ctx->src_comp[s];
     }
     a.src_val = ctx->step_in + (size_t)s_local * ctx->step_row;
+    a.err = ctx->err_flag;
     return a;
 }
 
@@ -462,13 +469,15 @@ template <typename R, bool STRICT, int NA>
 static void launch_step_t(php_ctx* ctx, int s_local, int& launches)
 {
     StepArgs<R> a = make_args<R>(ctx, s_local);
-    dim3 block(kBlockX, 8, 1);
-    dim3 grid((ctx->nx + kBlockX - 1) / kBlockX, (ctx->ny + 7) / 8, (ctx->nz + ctx->zchunk - 1) / ctx->zchunk);
+    dim3 block(kBlockX, kBlockY, 1);
+    dim3 grid((ctx->nx + kBlockX - 1) / kBlockX, (ctx->ny + kBlockY - 1) / kBlockY, (ctx->nz + ctx->zchunk - 1) / ctx->zchunk);
     prof_mark(ctx, s_local, 0, 0);
-    h_sweep<R, STRICT><<<grid, block, 0, ctx->stream>>>(a);
+    if (ctx->use_tma) h_sweep_tma<R, STRICT><<<grid, block, TmaGeom<R>::H_SMEM, ctx->stream>>>(a, ctx->maps);
+    else h_sweep<R, STRICT><<<grid, block, 0, ctx->stream>>>(a);
     prof_mark(ctx, s_local, 0, 1);
     prof_mark(ctx, s_local, 1, 0);
-    e_sweep<R, STRICT, NA><<<grid, block, 0, ctx->stream>>>(a);
+    if (ctx->use_tma) e_sweep_tma<R, STRICT, NA><<<grid, block, TmaGeom<R>::E_SMEM, ctx->stream>>>(a, ctx->maps);
+    else e_sweep<R, STRICT, NA><<<grid, block, 0, ctx->stream>>>(a);
     prof_mark(ctx, s_local, 1, 1);
     launches += 2;
     if (ctx->probe) {
@@ -496,25 +505,88 @@ static void launch_step_t(php_ctx* ctx, int s_local, int& launches)
 }
 
 typedef void (*step_fn)(php_ctx*, int, int&);
+typedef int (*prep_fn)(php_ctx*);
+
+/* the TMA sweeps need more than the default 48 KB of dynamic shared memory */
+template <typename R, bool STRICT, int NA>
+static int prepare_t(php_ctx* ctx)
+{
+    cudaError_t e = cudaFuncSetAttribute(h_sweep_tma<R, STRICT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)TmaGeom<R>::H_SMEM);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(e_sweep_tma<R, STRICT, NA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)TmaGeom<R>::E_SMEM);
+    if (e != cudaSuccess) return fail(ctx, PHP_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+    return PHP_OK;
+}
+
+struct StepKernels {
+    step_fn launch;
+    prep_fn prepare;
+};
 
 template <typename R, bool STRICT>
-static step_fn pick_na(int namax)
+static StepKernels pick_na(int namax)
 {
     switch (namax) {
-    case 0: return launch_step_t<R, STRICT, 0>;
-    case 2: return launch_step_t<R, STRICT, 2>;
-    case 4: return launch_step_t<R, STRICT, 4>;
-    case 8: return launch_step_t<R, STRICT, 8>;
-    case 16: return launch_step_t<R, STRICT, 16>;
-    default: return launch_step_t<R, STRICT, 64>;
+    case 0: return {launch_step_t<R, STRICT, 0>, prepare_t<R, STRICT, 0>};
+    case 2: return {launch_step_t<R, STRICT, 2>, prepare_t<R, STRICT, 2>};
+    case 4: return {launch_step_t<R, STRICT, 4>, prepare_t<R, STRICT, 4>};
+    case 8: return {launch_step_t<R, STRICT, 8>, prepare_t<R, STRICT, 8>};
+    case 16: return {launch_step_t<R, STRICT, 16>, prepare_t<R, STRICT, 16>};
+    default: return {launch_step_t<R, STRICT, 64>, prepare_t<R, STRICT, 64>};
     }
 }
 
-static step_fn pick_step(const php_ctx* ctx)
+static StepKernels pick_step(const php_ctx* ctx)
 {
     if (ctx->prec == PHP_PREC_FP64_STRICT) return pick_na<double, true>(ctx->namax_tpl);
     if (ctx->prec == PHP_PREC_FP64) return pick_na<double, false>(ctx->namax_tpl);
     return pick_na<float, false>(ctx->namax_tpl);
+}
+
+/* ------------------------------------------------------------ tensor maps */
+
+static int encode_map(php_ctx* ctx, CUtensorMap* m, void* base, CUtensorMapDataType dt, size_t esize, uint64_t d0,
+                      uint64_t d1, uint64_t d2, uint32_t b0, uint32_t b1)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn ||
+            q != cudaDriverEntryPointSuccess)
+            return fail(ctx, PHP_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    const cuuint64_t dims[3] = {d0, d1, d2};
+    const cuuint64_t strides[2] = {d0 * esize, d0 * d1 * esize};
+    const cuuint32_t box[3] = {b0, b1, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = encode(m, dt, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(ctx, PHP_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return PHP_OK;
+}
+
+/* Maps of the field arrays (planes -1..nz) and the material ids (planes
+ * 0..nz-1) with the boxes of php_sweeps_tma.cuh. */
+template <typename R>
+static int make_maps(php_ctx* ctx)
+{
+    using G = TmaGeom<R>;
+    const CUtensorMapDataType dt = sizeof(R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    const uint64_t nxp = ctx->nxp, ny = ctx->ny, nzh = ctx->nz + 2;
+    auto base = [&](int q) { return (void*)((char*)ctx->f[q] - (size_t)ctx->plane * sizeof(R)); };
+    int rc = PHP_OK;
+    for (int q = 0; q < 3 && !rc; ++q) {
+        rc = encode_map(ctx, &ctx->maps.e_halo[q], base(PHP_EX + q), dt, sizeof(R), nxp, ny, nzh, G::BX, G::BY);
+        if (!rc) rc = encode_map(ctx, &ctx->maps.h_own[q], base(PHP_HX + q), dt, sizeof(R), nxp, ny, nzh, G::TX, G::TY);
+        if (!rc) rc = encode_map(ctx, &ctx->maps.h_halo[q], base(PHP_HX + q), dt, sizeof(R), nxp, ny, nzh, G::BX, G::BY);
+        if (!rc) rc = encode_map(ctx, &ctx->maps.d_own[q], base(PHP_DX + q), dt, sizeof(R), nxp, ny, nzh, G::TX, G::TY);
+    }
+    if (!rc) rc = encode_map(ctx, &ctx->maps.mat, ctx->mat, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, nxp, ny, ctx->nz, G::TX, G::TY);
+    return rc;
 }
 
 /* --------------------------------------------------------------- creation */
@@ -725,6 +797,17 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
     else rc = upload_tables<double>(ctx, mats, ion_off, ion_coef, axes);
     if (rc) return rc;
 
+    /* sweep kernels: the TMA plane pipeline unless PHP_SWEEP=prefetch asks
+     * for the register-prefetch kernels (kept for A/B timing) */
+    const char* sw = getenv("PHP_SWEEP");
+    ctx->use_tma = !(sw && !strcmp(sw, "prefetch"));
+    if ((rc = dalloc(ctx, (void**)&ctx->err_flag, sizeof(int32_t)))) return rc;
+    if (ctx->use_tma) {
+        rc = ctx->prec == PHP_PREC_FP32 ? make_maps<float>(ctx) : make_maps<double>(ctx);
+        if (!rc) rc = pick_step(ctx).prepare(ctx);
+        if (rc) return rc;
+    }
+
     /* per-step inputs, scratch, staging */
     ctx->step_row = std::max(1, ctx->nsrc_active);
     if ((rc = dalloc(ctx, (void**)&ctx->step_in, (size_t)kMaxChunk * ctx->step_row * sizeof(double)))) return rc;
@@ -747,7 +830,7 @@ static int ensure_graph(php_ctx* ctx, int n, cudaGraphExec_t* out)
         *out = it->second;
         return PHP_OK;
     }
-    step_fn fn = pick_step(ctx);
+    step_fn fn = pick_step(ctx).launch;
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     int launches = 0;
@@ -891,6 +974,9 @@ int php_sync(php_ctx* ctx)
     if (!ctx) return PHP_ERR_INPUT;
     CK(cudaStreamSynchronize(ctx->stream));
     CK(cudaGetLastError());
+    int32_t flag = 0;
+    CK(cudaMemcpy(&flag, ctx->err_flag, sizeof(flag), cudaMemcpyDeviceToHost));
+    if (flag) return fail(ctx, PHP_ERR_TIMEOUT, "a sweep kernel gave up waiting for its plane loads");
     return PHP_OK;
 }
 

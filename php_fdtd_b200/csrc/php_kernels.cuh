@@ -105,6 +105,7 @@ struct StepArgs {
     int64_t src_cell[kMaxSources];
     int32_t src_comp[kMaxSources];
     const double* src_val;     /* nsrc values of this step */
+    int32_t* err;              /* set to 1 by a block whose bounded wait gave up */
 };
 
 /* ------------------------------------------------------------ arithmetic */
@@ -326,3 +327,4 @@ __global__ void __launch_bounds__(256) diag_pass2(const DiagPartial* scratch, in
 } // namespace phpdev
 
 #include "php_sweeps.cuh"
+#include "php_sweeps_tma.cuh"

@@ -252,16 +252,12 @@ __device__ __forceinline__ void rot_back(int flags, R cs, R sn, R& u0, R& u1, R&
     }
 }
 
-/* D sweep (fdtd.c:3238-3343) for one interior cell. */
+/* D sweep (fdtd.c:3238-3343) for one interior cell; hx0..hz0 are H at the
+ * cell, hxk/hyk at k-1, hz_jm/hx_jm at j-1, hz_im/hy_im at i-1. */
 template <typename R, bool STRICT>
-__device__ __forceinline__ void d_update(const StepArgs<R>& a, int i, int j, int k, int c, int sx, int sy,
-                                         R hx0, R hy0, R hz0, R hxk, R hyk, R& dx, R& dy, R& dz)
+__device__ __forceinline__ void d_update(const StepArgs<R>& a, int i, int j, int k, int sx, int sy, R hx0, R hy0,
+                                         R hz0, R hxk, R hyk, R hz_jm, R hx_jm, R hz_im, R hy_im, R& dx, R& dy, R& dz)
 {
-    const R* __restrict__ hxp = a.f.hx;
-    const R* __restrict__ hyp = a.f.hy;
-    const R* __restrict__ hzp = a.f.hz;
-    const R hz_jm = ldg(hzp + c - a.nxp), hx_jm = ldg(hxp + c - a.nxp);
-    const R hz_im = ldg(hzp + c - 1), hy_im = ldg(hyp + c - 1);
     const int L2 = 2 * a.L;
     const int sz = ldg_nh(a.tz.slot + k);
     if constexpr (STRICT) {
@@ -503,6 +499,66 @@ __device__ __forceinline__ void e_update(const StepArgs<R>& a, const MatCoef<R>&
     ez = nc;
 }
 
+/* One cell of the fused sweep once its H values are known: D update on
+ * the interior with the lossy eps'' term (fdtd.c:3238-3356), the sources of
+ * this step (fdtd.c:3363-3396), D -> E / ADE / ions (fdtd.c:3404-3528); D and E
+ * are stored to global memory. */
+template <typename R, bool STRICT, int NAMAX>
+__device__ __forceinline__ void e_cell(const StepArgs<R>& a, int i, int j, int k, int c, bool interior, int sx, int sy,
+                                       R hx0, R hy0, R hz0, R hxk, R hyk, R hz_jm, R hx_jm, R hz_im, R hy_im, R dx, R dy,
+                                       R dz, int mid)
+{
+    R* __restrict__ dxp = a.f.dx;
+    R* __restrict__ dyp = a.f.dy;
+    R* __restrict__ dzp = a.f.dz;
+    R* __restrict__ exp_ = a.f.ex;
+    R* __restrict__ eyp = a.f.ey;
+    R* __restrict__ ezp = a.f.ez;
+    const MatCoef<R>& m = a.mc[mid];
+    const int flags = m.flags;
+    R ex = R(0), ey = R(0), ez = R(0);
+    if (flags & (kLossy | kAde)) { ex = exp_[c]; ey = eyp[c]; ez = ezp[c]; }
+    if (interior) {
+        d_update<R, STRICT>(a, i, j, k, sx, sy, hx0, hy0, hz0, hxk, hyk, hz_jm, hx_jm, hz_im, hy_im, dx, dy, dz);
+        if (flags & kLossy) { /* fdtd.c:3349-3353 */
+            const R* q = m.eps_im;
+            if constexpr (STRICT) {
+                dx = SOp::sub(dx, SOp::mul(SOp::mul(a.c1, SOp::add(SOp::add(SOp::mul(q[0], ex), SOp::mul(q[1], ey)), SOp::mul(q[2], ez))), a.eps0));
+                dy = SOp::sub(dy, SOp::mul(SOp::mul(a.c1, SOp::add(SOp::add(SOp::mul(q[3], ex), SOp::mul(q[4], ey)), SOp::mul(q[5], ez))), a.eps0));
+                dz = SOp::sub(dz, SOp::mul(SOp::mul(a.c1, SOp::add(SOp::add(SOp::mul(q[6], ex), SOp::mul(q[7], ey)), SOp::mul(q[8], ez))), a.eps0));
+            } else {
+                dx -= q[0] * ex + q[1] * ey + q[2] * ez;
+                dy -= q[3] * ex + q[4] * ey + q[5] * ez;
+                dz -= q[6] * ex + q[7] * ey + q[8] * ez;
+            }
+        }
+    }
+    /* sources, in source order (fdtd.c:3363-3396) */
+    for (int s = 0; s < a.nsrc; ++s) {
+        if (a.src_cell[s] == c) {
+            const double v = a.src_val[s];
+            if constexpr (STRICT) {
+                const double add = SOp::mul(v, a.dt);
+                if (a.src_comp[s] == 0) dx = SOp::add(dx, add);
+                else if (a.src_comp[s] == 1) dy = SOp::add(dy, add);
+                else if (a.src_comp[s] == 2) dz = SOp::add(dz, add);
+            } else {
+                const R add = R(v * a.dt);
+                if (a.src_comp[s] == 0) dx += add;
+                else if (a.src_comp[s] == 1) dy += add;
+                else if (a.src_comp[s] == 2) dz += add;
+            }
+        }
+    }
+    dxp[c] = dx;
+    dyp[c] = dy;
+    dzp[c] = dz;
+    e_update<R, STRICT, NAMAX>(a, m, c, dx, dy, dz, ex, ey, ez);
+    exp_[c] = ex;
+    eyp[c] = ey;
+    ezp[c] = ez;
+}
+
 template <typename R>
 struct EIn {
     R hx, hy, hz, dx, dy, dz;
@@ -546,9 +602,6 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : PHP_E_MINB
     R* __restrict__ dxp = a.f.dx;
     R* __restrict__ dyp = a.f.dy;
     R* __restrict__ dzp = a.f.dz;
-    R* __restrict__ exp_ = a.f.ex;
-    R* __restrict__ eyp = a.f.ey;
-    R* __restrict__ ezp = a.f.ez;
     const uint8_t* __restrict__ mat = a.mat;
 
     R hxk = ldg(hx + c - P), hyk = ldg(hy + c - P); /* plane k-1 */
@@ -562,50 +615,15 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : PHP_E_MINB
 #else
         if (k > k0) e_fetch(cur, hx, hy, hz, dxp, dyp, dzp, mat, c);
 #endif
-        const MatCoef<R>& m = a.mc[cur.mid];
-        const int flags = m.flags;
-        R dx = cur.dx, dy = cur.dy, dz = cur.dz;
-        R ex = R(0), ey = R(0), ez = R(0);
-        if (flags & (kLossy | kAde)) { ex = exp_[c]; ey = eyp[c]; ez = ezp[c]; }
+        R hz_jm = R(0), hx_jm = R(0), hz_im = R(0), hy_im = R(0);
         if (interior) {
-            d_update<R, STRICT>(a, i, j, k, c, sx, sy, cur.hx, cur.hy, cur.hz, hxk, hyk, dx, dy, dz);
-            if (flags & kLossy) { /* fdtd.c:3349-3353 */
-                const R* q = m.eps_im;
-                if constexpr (STRICT) {
-                    dx = SOp::sub(dx, SOp::mul(SOp::mul(a.c1, SOp::add(SOp::add(SOp::mul(q[0], ex), SOp::mul(q[1], ey)), SOp::mul(q[2], ez))), a.eps0));
-                    dy = SOp::sub(dy, SOp::mul(SOp::mul(a.c1, SOp::add(SOp::add(SOp::mul(q[3], ex), SOp::mul(q[4], ey)), SOp::mul(q[5], ez))), a.eps0));
-                    dz = SOp::sub(dz, SOp::mul(SOp::mul(a.c1, SOp::add(SOp::add(SOp::mul(q[6], ex), SOp::mul(q[7], ey)), SOp::mul(q[8], ez))), a.eps0));
-                } else {
-                    dx -= q[0] * ex + q[1] * ey + q[2] * ez;
-                    dy -= q[3] * ex + q[4] * ey + q[5] * ez;
-                    dz -= q[6] * ex + q[7] * ey + q[8] * ez;
-                }
-            }
+            hz_jm = ldg(hz + c - a.nxp);
+            hx_jm = ldg(hx + c - a.nxp);
+            hz_im = ldg(hz + c - 1);
+            hy_im = ldg(hy + c - 1);
         }
-        /* sources, in source order (fdtd.c:3363-3396) */
-        for (int s = 0; s < a.nsrc; ++s) {
-            if (a.src_cell[s] == c) {
-                const double v = a.src_val[s];
-                if constexpr (STRICT) {
-                    const double add = SOp::mul(v, a.dt);
-                    if (a.src_comp[s] == 0) dx = SOp::add(dx, add);
-                    else if (a.src_comp[s] == 1) dy = SOp::add(dy, add);
-                    else if (a.src_comp[s] == 2) dz = SOp::add(dz, add);
-                } else {
-                    const R add = R(v * a.dt);
-                    if (a.src_comp[s] == 0) dx += add;
-                    else if (a.src_comp[s] == 1) dy += add;
-                    else if (a.src_comp[s] == 2) dz += add;
-                }
-            }
-        }
-        dxp[c] = dx;
-        dyp[c] = dy;
-        dzp[c] = dz;
-        e_update<R, STRICT, NAMAX>(a, m, c, dx, dy, dz, ex, ey, ez);
-        exp_[c] = ex;
-        eyp[c] = ey;
-        ezp[c] = ez;
+        e_cell<R, STRICT, NAMAX>(a, i, j, k, c, interior, sx, sy, cur.hx, cur.hy, cur.hz, hxk, hyk, hz_jm, hx_jm, hz_im,
+                                 hy_im, cur.dx, cur.dy, cur.dz, cur.mid);
         hxk = cur.hx;
         hyk = cur.hy;
 #if PHP_PREFETCH

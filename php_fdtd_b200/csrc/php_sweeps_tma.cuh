@@ -1,0 +1,395 @@
+/*
+ * php_sweeps_tma.cuh -- the two sweeps with a TMA plane pipeline (sm_100a).
+ *
+ * A block owns a 32 x 8 (x, y) tile of a z chunk.  One thread streams whole
+ * planes of the tile into a ring of kTmaStages shared-memory stages with
+ * cp.async.bulk.tensor (tile mode, no multicast: every byte comes from this
+ * GPU's own memory), each stage completed on its own mbarrier; all 256
+ * threads compute from shared memory.  The bytes in flight are set by the
+ * ring depth instead of by registers, which is what a streaming stencil on
+ * HBM needs.
+ *
+ *   h_sweep_tma: per plane, Ex/Ey/Ez with a +1 halo in x and y (the box is
+ *     widened to 16 bytes in x) and Hx/Hy/Hz of the tile; the update at k
+ *     reads E planes k and k+1.
+ *   e_sweep_tma: per plane, Hx/Hy/Hz with a -1 halo in x and y (the box starts
+ *     16 bytes left of the tile so that its x offset stays 16-byte aligned),
+ *     Dx/Dy/Dz and the material ids of the tile; the update at k reads H planes
+ *     k and k-1.
+ * Out-of-range parts of a box read the tensor map's zero fill; those values
+ * are only used by cells the reference never updates there (i = nx-1 or
+ * j = ny-1 for H, the x/y border for D).
+ *
+ * Waits on the mbarriers are bounded: after kWaitLimit polls the block sets
+ * a device error flag and leaves the loop (the decision is made uniform
+ * across the block with __syncthreads_or), and the host reports
+ * PHP_ERR_TIMEOUT.
+ */
+#pragma once
+
+#include <cuda.h>
+
+namespace phpdev {
+
+constexpr int kTmaStages = 4;
+constexpr uint32_t kWaitLimit = 1u << 24;
+
+/* Tensor maps of the device arrays (3-D: x, y, plane; planes count from the
+ * low halo plane of the field arrays). */
+struct TmaMaps {
+    CUtensorMap e_halo[3]; /* Ex, Ey, Ez: box (32 + 16/s) x 9 at (i0, j0) */
+    CUtensorMap h_own[3];  /* Hx, Hy, Hz: box 32 x 8 */
+    CUtensorMap h_halo[3]; /* Hx, Hy, Hz: box (32 + 16/s) x 9 at (i0 - 16/s, j0 - 1) */
+    CUtensorMap d_own[3];  /* Dx, Dy, Dz: box 32 x 8 */
+    CUtensorMap mat;       /* uint8 ids (no halo planes): box 32 x 8 */
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t done;
+    asm volatile(
+        "{\n"
+        "  .reg .pred p;\n"
+        "  mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        "  selp.u32 %0, 1, 0, p;\n"
+        "}\n"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+/* bounded wait: false after kWaitLimit polls */
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+{
+    for (uint32_t n = 0; n < kWaitLimit; ++n)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void fence_barrier_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+/* orders this thread's generic-proxy accesses to shared memory before the
+ * async-proxy (TMA) writes it issues next */
+__device__ __forceinline__ void fence_proxy_async_smem()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y, int z)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
+        ::"r"(smem_addr(dst)), "l"(map), "r"(smem_addr(bar)), "r"(x), "r"(y), "r"(z)
+        : "memory");
+}
+
+template <typename R>
+struct TmaGeom {
+    static constexpr int TX = kBlockX, TY = kBlockY;
+    static constexpr int HALO = 16 / (int)sizeof(R);      /* x halo widened to 16 bytes */
+    static constexpr int BX = TX + HALO, BY = TY + 1;      /* halo box */
+    static constexpr int HALO_ELEMS = BX * BY, OWN_ELEMS = TX * TY;
+    static constexpr uint32_t HALO_BYTES = HALO_ELEMS * sizeof(R), OWN_BYTES = OWN_ELEMS * sizeof(R);
+    static constexpr uint32_t MAT_BYTES = OWN_ELEMS;
+    __host__ __device__ static constexpr uint32_t align128(uint32_t b) { return (b + 127u) / 128u * 128u; }
+    /* H sweep stage: 3 halo E boxes + 3 own H boxes */
+    static constexpr uint32_t H_STAGE = align128(3 * align128(HALO_BYTES) + 3 * align128(OWN_BYTES));
+    /* E sweep stage: 3 halo H boxes + 3 own D boxes + material ids */
+    static constexpr uint32_t E_STAGE = align128(3 * align128(HALO_BYTES) + 3 * align128(OWN_BYTES) + align128(MAT_BYTES));
+    /* dynamic shared memory: 128 bytes of alignment slack, the stages, then
+     * the stage barriers */
+    static constexpr uint32_t H_SMEM = 128 + kTmaStages * H_STAGE + kTmaStages * 8;
+    static constexpr uint32_t E_SMEM = 128 + kTmaStages * E_STAGE + kTmaStages * 8;
+};
+
+/* 128-byte aligned start of the stage ring inside dynamic shared memory */
+__device__ __forceinline__ unsigned char* ring_base(unsigned char* dyn)
+{
+    const uint32_t a = smem_addr(dyn);
+    return dyn + ((128u - (a & 127u)) & 127u);
+}
+
+/* ================================================================ H sweep */
+
+/* fdtd.c:3123-3231: cells i < nx-1, j < ny-1, all k. */
+template <typename R, bool STRICT>
+__global__ void __launch_bounds__(kBlockX * kBlockY) h_sweep_tma(const __grid_constant__ StepArgs<R> a,
+                                                                 const __grid_constant__ TmaMaps tm)
+{
+    using G = TmaGeom<R>;
+    extern __shared__ __align__(128) unsigned char dyn_smem[];
+    unsigned char* smem = ring_base(dyn_smem);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + kTmaStages * G::H_STAGE);
+
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * G::TX + tx;
+    const int i0 = blockIdx.x * G::TX, j0 = blockIdx.y * G::TY;
+    const int i = i0 + tx, j = j0 + ty;
+    const int k0 = blockIdx.z * a.zchunk;
+    const int k1 = min(k0 + a.zchunk, a.nz);
+    if (k0 >= k1) return; /* uniform over the block */
+
+    constexpr uint32_t EB = G::align128(G::HALO_BYTES), HB = G::align128(G::OWN_BYTES);
+    auto stage = [&](int p) -> unsigned char* { return smem + (uint32_t)((p - k0) % kTmaStages) * G::H_STAGE; };
+    /* plane p = k0..k1: E (halo boxes) of every plane, H of planes < k1 */
+    auto issue = [&](int p) {
+        uint64_t* bar = &full[(p - k0) % kTmaStages];
+        unsigned char* b = stage(p);
+        const bool with_h = p < k1;
+        mbar_arrive_expect_tx(bar, 3 * G::HALO_BYTES + (with_h ? 3 * G::OWN_BYTES : 0u));
+        for (int q = 0; q < 3; ++q) tma_load_3d(b + q * EB, &tm.e_halo[q], bar, i0, j0, p + 1);
+        if (with_h)
+            for (int q = 0; q < 3; ++q) tma_load_3d(b + 3 * EB + q * HB, &tm.h_own[q], bar, i0, j0, p + 1);
+    };
+
+    if (tid == 0) {
+        for (int s = 0; s < kTmaStages; ++s) mbar_init(&full[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (tid == 0)
+        for (int p = k0; p <= min(k1, k0 + kTmaStages - 1); ++p) issue(p);
+
+    const bool active = (i < a.nx - 1) && (j < a.ny - 1);
+    const int L2 = 2 * a.L;
+    const int nxp = a.nxp, ny = a.ny;
+    const int sx = active ? ldg(a.tx.slot + i) : -1;
+    const int sy = active ? ldg(a.ty.slot + j) : -1;
+    R khx = R(0), khy = R(0);
+    if constexpr (!STRICT) {
+        if (active) {
+            khx = ldg(a.tx.kh + i);
+            khy = ldg(a.ty.kh + j);
+        }
+    }
+    R* __restrict__ hxg = a.f.hx;
+    R* __restrict__ hyg = a.f.hy;
+    R* __restrict__ hzg = a.f.hz;
+    const int eo = ty * G::BX + tx; /* own cell in a halo box */
+    const int ho = ty * G::TX + tx; /* own cell in an own box */
+
+    for (int k = k0; k < k1; ++k) {
+        bool ok = true;
+        if (k == k0) ok = mbar_wait(&full[0], 0);
+        ok = ok && mbar_wait(&full[(k + 1 - k0) % kTmaStages], ((k + 1 - k0) / kTmaStages) & 1);
+        if (ok && active) {
+            const unsigned char* b0 = stage(k);
+            const unsigned char* b1 = stage(k + 1);
+            const R* Ex0 = reinterpret_cast<const R*>(b0);
+            const R* Ey0 = reinterpret_cast<const R*>(b0 + EB);
+            const R* Ez0 = reinterpret_cast<const R*>(b0 + 2 * EB);
+            const R* Ex1 = reinterpret_cast<const R*>(b1);
+            const R* Ey1 = reinterpret_cast<const R*>(b1 + EB);
+            const R* Hx0 = reinterpret_cast<const R*>(b0 + 3 * EB);
+            const R* Hy0 = reinterpret_cast<const R*>(b0 + 3 * EB + HB);
+            const R* Hz0 = reinterpret_cast<const R*>(b0 + 3 * EB + 2 * HB);
+            const R ex0 = Ex0[eo], ey0 = Ey0[eo], ez0 = Ez0[eo];
+            const R ex1 = Ex1[eo], ey1 = Ey1[eo];
+            const R ezi = Ez0[eo + 1], eyi = Ey0[eo + 1];
+            const R ezj = Ez0[eo + G::BX], exj = Ex0[eo + G::BX];
+            const R hx0 = Hx0[ho], hy0 = Hy0[ho], hz0 = Hz0[ho];
+            const int c = (k * ny + j) * nxp + i;
+            const int sz = ldg_nh(a.tz.slot + k);
+            if constexpr (STRICT) {
+                const double mu0 = a.mu0;
+                /* fdtd.c:3132-3137 */
+                const double dEy_dz = SOp::div(SOp::sub(ey1, ey0), a.dzs);
+                const double dEz_dy = SOp::div(SOp::sub(ezj, ez0), a.dys);
+                const double dEz_dx = SOp::div(SOp::sub(ezi, ez0), a.dxs);
+                const double dEx_dz = SOp::div(SOp::sub(ex1, ex0), a.dzs);
+                const double dEx_dy = SOp::div(SOp::sub(exj, ex0), a.dys);
+                const double dEy_dx = SOp::div(SOp::sub(eyi, ey0), a.dxs);
+                double pxy = 0.0, pxz = 0.0, pyx = 0.0, pyz = 0.0, pzx = 0.0, pzy = 0.0;
+                double kappa_x = 1.0, kappa_y = 1.0, kappa_z = 1.0;
+                if (sx >= 0) { /* fdtd.c:3143-3170 */
+                    kappa_x = ldg_nh(a.tx.kappa + i);
+                    const double bb = ldg_nh(a.tx.b + i), cc = ldg_nh(a.tx.c + i);
+                    const int q = (k * ny + j) * L2 + sx;
+                    pxy = a.psi.hxy[q];
+                    pxz = a.psi.hxz[q];
+                    a.psi.hxy[q] = SOp::add(SOp::mul(bb, pxy), SOp::mul(cc, SOp::div(dEz_dx, mu0)));
+                    a.psi.hxz[q] = SOp::add(SOp::mul(bb, pxz), SOp::mul(cc, SOp::div(-dEy_dx, mu0)));
+                }
+                if (sy >= 0) { /* fdtd.c:3173-3200 */
+                    kappa_y = ldg_nh(a.ty.kappa + j);
+                    const double bb = ldg_nh(a.ty.b + j), cc = ldg_nh(a.ty.c + j);
+                    const int q = (k * L2 + sy) * nxp + i;
+                    pyx = a.psi.hyx[q];
+                    pyz = a.psi.hyz[q];
+                    a.psi.hyx[q] = SOp::add(SOp::mul(bb, pyx), SOp::mul(cc, SOp::div(-dEz_dy, mu0)));
+                    a.psi.hyz[q] = SOp::add(SOp::mul(bb, pyz), SOp::mul(cc, SOp::div(dEx_dy, mu0)));
+                }
+                int qz = 0;
+                if (sz >= 0) { /* fdtd.c:3203-3219 */
+                    kappa_z = ldg_nh(a.tz.kappa + k);
+                    qz = (sz * ny + j) * nxp + i;
+                    pzx = a.psi.hzx[qz];
+                    pzy = a.psi.hzy[qz];
+                }
+                /* fdtd.c:3222-3224 */
+                const double ux = SOp::add(SOp::add(SOp::add(SOp::div(SOp::div(-dEz_dy, mu0), kappa_y), pyx),
+                                                    SOp::div(SOp::div(dEy_dz, mu0), kappa_z)), pzx);
+                const double uy = SOp::add(SOp::add(SOp::add(SOp::div(SOp::div(dEz_dx, mu0), kappa_x), pxy),
+                                                    SOp::div(SOp::div(-dEx_dz, mu0), kappa_z)), pzy);
+                const double uz = SOp::add(SOp::add(SOp::add(SOp::div(SOp::div(-dEy_dx, mu0), kappa_x), pxz),
+                                                    SOp::div(SOp::div(dEx_dy, mu0), kappa_y)), pyz);
+                hxg[c] = SOp::add(hx0, SOp::mul(a.dt, ux));
+                hyg[c] = SOp::add(hy0, SOp::mul(a.dt, uy));
+                hzg[c] = SOp::add(hz0, SOp::mul(a.dt, uz));
+                if (sz >= 0) { /* fdtd.c:3225-3228 */
+                    const double bb = ldg_nh(a.tz.b + k), cc = ldg_nh(a.tz.c + k);
+                    a.psi.hzx[qz] = SOp::add(SOp::mul(bb, pzx), SOp::mul(cc, SOp::div(dEy_dz, mu0)));
+                    a.psi.hzy[qz] = SOp::add(SOp::mul(bb, pzy), SOp::mul(cc, SOp::div(-dEx_dz, mu0)));
+                }
+            } else {
+                const R dEyz = ey1 - ey0, dEzy = ezj - ez0, dEzx = ezi - ez0;
+                const R dExz = ex1 - ex0, dExy = exj - ex0, dEyx = eyi - ey0;
+                const R khz = ldg_nh(a.tz.kh + k);
+                R ux = -khy * dEzy + khz * dEyz;
+                R uy = khx * dEzx - khz * dExz;
+                R uz = -khx * dEyx + khy * dExy;
+                if (sx >= 0) {
+                    const R bb = ldg_nh(a.tx.b + i), ch = ldg_nh(a.tx.ch + i);
+                    const int q = (k * ny + j) * L2 + sx;
+                    const R pxy = a.psi.hxy[q], pxz = a.psi.hxz[q];
+                    uy += pxy;
+                    uz += pxz;
+                    a.psi.hxy[q] = bb * pxy + ch * dEzx;
+                    a.psi.hxz[q] = bb * pxz - ch * dEyx;
+                }
+                if (sy >= 0) {
+                    const R bb = ldg_nh(a.ty.b + j), ch = ldg_nh(a.ty.ch + j);
+                    const int q = (k * L2 + sy) * nxp + i;
+                    const R pyx = a.psi.hyx[q], pyz = a.psi.hyz[q];
+                    ux += pyx;
+                    uz += pyz;
+                    a.psi.hyx[q] = bb * pyx - ch * dEzy;
+                    a.psi.hyz[q] = bb * pyz + ch * dExy;
+                }
+                if (sz >= 0) {
+                    const R bb = ldg_nh(a.tz.b + k), ch = ldg_nh(a.tz.ch + k);
+                    const int q = (sz * ny + j) * nxp + i;
+                    const R pzx = a.psi.hzx[q], pzy = a.psi.hzy[q];
+                    ux += pzx;
+                    uy += pzy;
+                    a.psi.hzx[q] = bb * pzx + ch * dEyz;
+                    a.psi.hzy[q] = bb * pzy - ch * dExz;
+                }
+                hxg[c] = hx0 + ux;
+                hyg[c] = hy0 + uy;
+                hzg[c] = hz0 + uz;
+            }
+        }
+        /* every thread is done with plane k: its stage takes plane k + stages */
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicExch(a.err, 1);
+            break;
+        }
+        if (tid == 0 && k + kTmaStages <= k1) {
+            fence_proxy_async_smem();
+            issue(k + kTmaStages);
+        }
+    }
+}
+
+/* ================================================================ E sweep */
+
+/* fdtd.c:3238-3528 fused, as e_sweep, with H, D and the material ids
+ * streamed through the stage ring. */
+template <typename R, bool STRICT, int NAMAX>
+__global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : PHP_E_MINBLOCKS))
+    e_sweep_tma(const __grid_constant__ StepArgs<R> a, const __grid_constant__ TmaMaps tm)
+{
+    using G = TmaGeom<R>;
+    extern __shared__ __align__(128) unsigned char dyn_smem[];
+    unsigned char* smem = ring_base(dyn_smem);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + kTmaStages * G::E_STAGE);
+
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * G::TX + tx;
+    const int i0 = blockIdx.x * G::TX, j0 = blockIdx.y * G::TY;
+    const int i = i0 + tx, j = j0 + ty;
+    const int k0 = blockIdx.z * a.zchunk;
+    const int k1 = min(k0 + a.zchunk, a.nz);
+    if (k0 >= k1) return; /* uniform over the block */
+
+    constexpr uint32_t HB = G::align128(G::HALO_BYTES), OB = G::align128(G::OWN_BYTES);
+    /* plane p = k0-1 .. k1-1 into stage (p - k0 + 1) % stages */
+    auto stage = [&](int p) -> unsigned char* { return smem + (uint32_t)((p - k0 + 1) % kTmaStages) * G::E_STAGE; };
+    auto issue = [&](int p) {
+        uint64_t* bar = &full[(p - k0 + 1) % kTmaStages];
+        unsigned char* b = stage(p);
+        const bool own = p >= k0;
+        mbar_arrive_expect_tx(bar, 3 * G::HALO_BYTES + (own ? 3 * G::OWN_BYTES + G::MAT_BYTES : 0u));
+        for (int q = 0; q < 3; ++q) tma_load_3d(b + q * HB, &tm.h_halo[q], bar, i0 - G::HALO, j0 - 1, p + 1);
+        if (own) {
+            for (int q = 0; q < 3; ++q) tma_load_3d(b + 3 * HB + q * OB, &tm.d_own[q], bar, i0, j0, p + 1);
+            tma_load_3d(b + 3 * HB + 3 * OB, &tm.mat, bar, i0, j0, p);
+        }
+    };
+
+    if (tid == 0) {
+        for (int s = 0; s < kTmaStages; ++s) mbar_init(&full[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (tid == 0)
+        for (int p = k0 - 1; p <= min(k1 - 1, k0 - 1 + kTmaStages - 1); ++p) issue(p);
+
+    const bool active = (i < a.nx) && (j < a.ny);
+    const bool interior = (i >= 1 && i < a.nx - 1 && j >= 1 && j < a.ny - 1);
+    const int sx = active ? ldg(a.tx.slot + i) : -1;
+    const int sy = active ? ldg(a.ty.slot + j) : -1;
+    const int ho = (ty + 1) * G::BX + tx + G::HALO; /* own cell in a halo box */
+    const int oo = ty * G::TX + tx;                 /* own cell in an own box */
+
+    for (int k = k0; k < k1; ++k) {
+        bool ok = true;
+        if (k == k0) ok = mbar_wait(&full[0], 0);
+        ok = ok && mbar_wait(&full[(k - k0 + 1) % kTmaStages], ((k - k0 + 1) / kTmaStages) & 1);
+        if (ok && active) {
+            const unsigned char* bp = stage(k - 1);
+            const unsigned char* bc = stage(k);
+            const R* Hxp = reinterpret_cast<const R*>(bp);
+            const R* Hyp = reinterpret_cast<const R*>(bp + HB);
+            const R* Hx = reinterpret_cast<const R*>(bc);
+            const R* Hy = reinterpret_cast<const R*>(bc + HB);
+            const R* Hz = reinterpret_cast<const R*>(bc + 2 * HB);
+            const R* Dx = reinterpret_cast<const R*>(bc + 3 * HB);
+            const R* Dy = reinterpret_cast<const R*>(bc + 3 * HB + OB);
+            const R* Dz = reinterpret_cast<const R*>(bc + 3 * HB + 2 * OB);
+            const uint8_t* M = reinterpret_cast<const uint8_t*>(bc + 3 * HB + 3 * OB);
+            const int c = (k * a.ny + j) * a.nxp + i;
+            e_cell<R, STRICT, NAMAX>(a, i, j, k, c, interior, sx, sy, Hx[ho], Hy[ho], Hz[ho], Hxp[ho], Hyp[ho],
+                                     Hz[ho - G::BX], Hx[ho - G::BX], Hz[ho - 1], Hy[ho - 1], Dx[oo], Dy[oo], Dz[oo], M[oo]);
+        }
+        /* every thread is done with plane k-1: its stage takes plane k-1 + stages */
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicExch(a.err, 1);
+            break;
+        }
+        if (tid == 0 && k - 1 + kTmaStages <= k1 - 1) {
+            fence_proxy_async_smem();
+            issue(k - 1 + kTmaStages);
+        }
+    }
+}
+
+} // namespace phpdev
