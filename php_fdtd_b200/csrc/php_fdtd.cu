@@ -72,8 +72,13 @@ struct php_ctx {
     void* ion_coef = nullptr;
     void* axis_tab[3][7] = {};   /* kappa b c kh kd ch cd per axis */
     int32_t* axis_slot[3] = {};
-    double* step_in = nullptr;   /* [kMaxChunk][row] */
-    double* step_in_host = nullptr;
+    /* per-step inputs (source values, DFT flags and phasors), double
+     * buffered so that the host fills one while the GPU runs the other */
+    double* step_in = nullptr;   /* buffer the graph being recorded reads */
+    double* step_in_dev[2] = {};  /* [kMaxChunk][row] each */
+    double* step_in_host[2] = {}; /* pinned */
+    cudaEvent_t staged[2] = {};   /* copy out of step_in_host[b] finished */
+    int chunk_no = 0;
     int step_row = 0;
     void* scratch = nullptr;     /* plane gathers, diagnostics */
     size_t scratch_bytes = 0;
@@ -93,7 +98,7 @@ struct php_ctx {
 
     /* stepping */
     int32_t t = 0;
-    std::map<int, cudaGraphExec_t> graphs;
+    std::map<int, cudaGraphExec_t> graphs; /* key: 2 * steps + input buffer */
     int last_launches = 0;
 
     /* probe */
@@ -314,6 +319,12 @@ static MatCoef<R> pack_material(const php_ctx* ctx, const MatD& s, int ion_off)
     o.cs = (R)s.cs;
     o.sn = (R)s.sn;
     o.ade_scale = (R)((1.0 - s.lt) / (d.epsilon0 * kEpsInf));
+    if (!strict && !(s.flags & (kLossy | kAde | kRotZ | kRotX | kAtoms))) {
+        const double* e = s.eps_inv;
+        if (e[1] == 0.0 && e[2] == 0.0 && e[3] == 0.0 && e[5] == 0.0 && e[6] == 0.0 && e[7] == 0.0 && e[0] == e[4] &&
+            e[0] == e[8])
+            o.flags |= kIso;
+    }
     return o;
 }
 
@@ -433,6 +444,10 @@ static StepArgs<R> make_args(php_ctx* ctx, int s_local)
     a.r = (R*)ctx->r;
     a.v = (R*)ctx->v;
     a.nslot = ctx->nslot;
+#ifndef PHP_SMEM_MATS
+#define PHP_SMEM_MATS 0
+#endif
+    a.nmat = PHP_SMEM_MATS ? std::min(ctx->d.num_materials, kSmemMats) : 0;
     a.nx = ctx->nx;
     a.ny = ctx->ny;
     a.nz = ctx->nz;
@@ -476,7 +491,8 @@ static void launch_step_t(php_ctx* ctx, int s_local, int& launches)
     else h_sweep<R, STRICT><<<grid, block, 0, ctx->stream>>>(a);
     prof_mark(ctx, s_local, 0, 1);
     prof_mark(ctx, s_local, 1, 0);
-    if (ctx->use_tma) e_sweep_tma<R, STRICT, NA><<<grid, block, TmaGeom<R>::E_SMEM, ctx->stream>>>(a, ctx->maps);
+    if (ctx->use_tma)
+        e_sweep_tma<R, STRICT, NA><<<grid, block, TmaGeom<R>::E_SMEM + a.nmat * sizeof(MatCoef<R>), ctx->stream>>>(a, ctx->maps);
     else e_sweep<R, STRICT, NA><<<grid, block, 0, ctx->stream>>>(a);
     prof_mark(ctx, s_local, 1, 1);
     launches += 2;
@@ -515,7 +531,7 @@ static int prepare_t(php_ctx* ctx)
                                          (int)TmaGeom<R>::H_SMEM);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(e_sweep_tma<R, STRICT, NA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)TmaGeom<R>::E_SMEM);
+                                 (int)(TmaGeom<R>::E_SMEM + kSmemMats * sizeof(MatCoef<R>)));
     if (e != cudaSuccess) return fail(ctx, PHP_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
     return PHP_OK;
 }
@@ -636,9 +652,30 @@ static void ctx_free(php_ctx* ctx)
     for (cudaEvent_t e : ctx->prof_ev) cudaEventDestroy(e);
     ctx->prof_ev.clear();
     if (ctx->host_stage) cudaFreeHost(ctx->host_stage);
-    if (ctx->step_in_host) cudaFreeHost(ctx->step_in_host);
+    for (int b = 0; b < 2; ++b) {
+        if (ctx->step_in_host[b]) cudaFreeHost(ctx->step_in_host[b]);
+        if (ctx->staged[b]) cudaEventDestroy(ctx->staged[b]);
+    }
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
+}
+
+/* (Re)allocates both per-step input buffers for rows of `row` doubles; the
+ * stream must be idle.  Replaced device buffers stay allocated until
+ * destroy. */
+static int alloc_step_inputs(php_ctx* ctx, int row)
+{
+    ctx->step_row = row;
+    for (int b = 0; b < 2; ++b) {
+        int rc = dalloc(ctx, (void**)&ctx->step_in_dev[b], (size_t)kMaxChunk * row * sizeof(double));
+        if (rc) return rc;
+        if (ctx->step_in_host[b]) cudaFreeHost(ctx->step_in_host[b]);
+        ctx->step_in_host[b] = nullptr;
+        CK(cudaMallocHost((void**)&ctx->step_in_host[b], (size_t)kMaxChunk * row * sizeof(double)));
+        if (!ctx->staged[b]) CK(cudaEventCreateWithFlags(&ctx->staged[b], cudaEventDisableTiming));
+    }
+    ctx->step_in = ctx->step_in_dev[0];
+    return PHP_OK;
 }
 
 static int create_impl(const php_desc* desc, php_ctx* ctx)
@@ -809,9 +846,7 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
     }
 
     /* per-step inputs, scratch, staging */
-    ctx->step_row = std::max(1, ctx->nsrc_active);
-    if ((rc = dalloc(ctx, (void**)&ctx->step_in, (size_t)kMaxChunk * ctx->step_row * sizeof(double)))) return rc;
-    CK(cudaMallocHost((void**)&ctx->step_in_host, (size_t)kMaxChunk * ctx->step_row * sizeof(double)));
+    if ((rc = alloc_step_inputs(ctx, std::max(1, ctx->nsrc_active)))) return rc;
     const size_t maxplane = std::max({(size_t)nx * ny, (size_t)ny * nz, (size_t)nx * nz});
     ctx->scratch_bytes = std::max(maxplane * sizeof(double), (size_t)4096 * sizeof(DiagPartial));
     if ((rc = dalloc(ctx, &ctx->scratch, ctx->scratch_bytes))) return rc;
@@ -823,13 +858,16 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
 
 /* ---------------------------------------------------------------- stepping */
 
-static int ensure_graph(php_ctx* ctx, int n, cudaGraphExec_t* out)
+/* graph of n steps reading per-step input buffer b */
+static int ensure_graph(php_ctx* ctx, int n, int b, cudaGraphExec_t* out)
 {
-    auto it = ctx->graphs.find(n);
+    const int key = 2 * n + b;
+    auto it = ctx->graphs.find(key);
     if (it != ctx->graphs.end()) {
         *out = it->second;
         return PHP_OK;
     }
+    ctx->step_in = ctx->step_in_dev[b];
     step_fn fn = pick_step(ctx).launch;
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
@@ -846,7 +884,7 @@ static int ensure_graph(php_ctx* ctx, int n, cudaGraphExec_t* out)
     cudaError_t ie = cudaGraphInstantiate(&ge, g, 0);
     cudaGraphDestroy(g);
     if (ie != cudaSuccess) return fail(ctx, PHP_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ie));
-    ctx->graphs[n] = ge;
+    ctx->graphs[key] = ge;
     *out = ge;
     return PHP_OK;
 }
@@ -867,14 +905,7 @@ static int relayout_step_inputs(php_ctx* ctx)
     }
     if (row == ctx->step_row) return PHP_OK;
     drop_graphs(ctx);
-    /* the old buffers stay in the allocation list until destroy */
-    ctx->step_row = row;
-    int rc = dalloc(ctx, (void**)&ctx->step_in, (size_t)kMaxChunk * row * sizeof(double));
-    if (rc) return rc;
-    if (ctx->step_in_host) cudaFreeHost(ctx->step_in_host);
-    ctx->step_in_host = nullptr;
-    CK(cudaMallocHost((void**)&ctx->step_in_host, (size_t)kMaxChunk * row * sizeof(double)));
-    return PHP_OK;
+    return alloc_step_inputs(ctx, row);
 }
 
 template <typename R>
@@ -926,9 +957,11 @@ int php_step(php_ctx* ctx, int32_t nsteps)
     const double dt = ctx->d.dt;
     while (nsteps > 0) {
         const int n = std::min(nsteps, kMaxChunk);
-        /* wait until the previous chunk has consumed the staging buffer */
-        CK(cudaStreamSynchronize(ctx->stream));
-        double* h = ctx->step_in_host;
+        const int b = ctx->chunk_no & 1;
+        /* the copy out of this pinned buffer two chunks ago must be done;
+         * the chunk in between keeps the GPU busy meanwhile */
+        CK(cudaEventSynchronize(ctx->staged[b]));
+        double* h = ctx->step_in_host[b];
         for (int s = 0; s < n; s++) {
             const int t = ctx->t + s;
             double* row = h + (size_t)s * ctx->step_row;
@@ -946,11 +979,16 @@ int php_step(php_ctx* ctx, int32_t nsteps)
                 if (take) p.nsamples++;
             }
         }
-        CK(cudaMemcpyAsync(ctx->step_in, h, (size_t)n * ctx->step_row * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        /* the device buffer b was last read by the graph two chunks back,
+         * which precedes this copy on the stream */
+        CK(cudaMemcpyAsync(ctx->step_in_dev[b], h, (size_t)n * ctx->step_row * sizeof(double), cudaMemcpyHostToDevice,
+                           ctx->stream));
+        CK(cudaEventRecord(ctx->staged[b], ctx->stream));
         cudaGraphExec_t g;
-        int rc = ensure_graph(ctx, n, &g);
+        int rc = ensure_graph(ctx, n, b, &g);
         if (rc) return rc;
         CK(cudaGraphLaunch(g, ctx->stream));
+        ctx->chunk_no++;
         if (ctx->profile) {
             CK(cudaStreamSynchronize(ctx->stream));
             for (int s = 0; s < n; s++)

@@ -56,7 +56,12 @@ struct MatCoef {
     R pad2;
 };
 
-enum : int32_t { kLossy = 1, kAde = 2, kRotZ = 4, kRotX = 8, kAtoms = 16 };
+/* kIso (fast modes only): no rotation, loss, ADE or atoms and eps^-1 a
+ * multiple of the identity, so E = eps_inv[0] * D. */
+enum : int32_t { kLossy = 1, kAde = 2, kRotZ = 4, kRotX = 8, kAtoms = 16, kIso = 32 };
+
+/* materials the fused sweep keeps in shared memory (ids above read global) */
+constexpr int kSmemMats = 16;
 
 /* Per-axis CPML tables, indexed by the cell index along the axis.  slot < 0
  * outside the PML.  Strict uses kappa, b, c (fdtd.c:3146-3151 evaluated on
@@ -96,6 +101,7 @@ struct StepArgs {
     const R* ion_coef;
     R *P, *Po, *r, *v;         /* pools */
     int64_t nslot;
+    int32_t nmat;
     int32_t nx, ny, nz, nxp, L, zchunk;
     int64_t plane;             /* nxp * ny */
     /* strict scalars */

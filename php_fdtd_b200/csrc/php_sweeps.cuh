@@ -252,14 +252,50 @@ __device__ __forceinline__ void rot_back(int flags, R cs, R sn, R& u0, R& u1, R&
     }
 }
 
-/* D sweep (fdtd.c:3238-3343) for one interior cell; hx0..hz0 are H at the
- * cell, hxk/hyk at k-1, hz_jm/hx_jm at j-1, hz_im/hy_im at i-1. */
-template <typename R, bool STRICT>
-__device__ __forceinline__ void d_update(const StepArgs<R>& a, int i, int j, int k, int sx, int sy, R hx0, R hy0,
-                                         R hz0, R hxk, R hyk, R hz_jm, R hx_jm, R hz_im, R hy_im, R& dx, R& dy, R& dz)
+/* CPML state of one cell read before its update: the z slot of the plane
+ * and the old psi values of every PML axis the cell lies in (zero
+ * elsewhere).  Loading them apart from the update lets a kernel issue these
+ * loads early, before it waits for the plane's other inputs. */
+template <typename R>
+struct CellPsi {
+    int sz;
+    R xy, xz, yx, yz, zx, zy;
+};
+
+/* psi_D of fdtd.c:3258-3334 (the reads) */
+template <typename R>
+__device__ __forceinline__ void load_psi_d(const StepArgs<R>& a, int i, int j, int k, int sx, int sy, CellPsi<R>& ps)
 {
     const int L2 = 2 * a.L;
-    const int sz = ldg_nh(a.tz.slot + k);
+    ps.sz = ldg_nh(a.tz.slot + k);
+    ps.xy = ps.xz = ps.yx = ps.yz = ps.zx = ps.zy = R(0);
+    if (sx >= 0) {
+        const int q = (k * a.ny + j) * L2 + sx;
+        ps.xy = a.psi.dxy[q];
+        ps.xz = a.psi.dxz[q];
+    }
+    if (sy >= 0) {
+        const int q = (k * L2 + sy) * a.nxp + i;
+        ps.yx = a.psi.dyx[q];
+        ps.yz = a.psi.dyz[q];
+    }
+    if (ps.sz >= 0) {
+        const int q = (ps.sz * a.ny + j) * a.nxp + i;
+        ps.zx = a.psi.dzx[q];
+        ps.zy = a.psi.dzy[q];
+    }
+}
+
+/* D sweep (fdtd.c:3238-3343) for one interior cell; hx0..hz0 are H at the
+ * cell, hxk/hyk at k-1, hz_jm/hx_jm at j-1, hz_im/hy_im at i-1; ps holds the
+ * old psi values (load_psi_d). */
+template <typename R, bool STRICT>
+__device__ __forceinline__ void d_update(const StepArgs<R>& a, int i, int j, int k, int sx, int sy, R hx0, R hy0,
+                                         R hz0, R hxk, R hyk, R hz_jm, R hx_jm, R hz_im, R hy_im,
+                                         const CellPsi<R>& ps, R& dx, R& dy, R& dz)
+{
+    const int L2 = 2 * a.L;
+    const int sz = ps.sz;
     if constexpr (STRICT) {
         const double dHz_dy = SOp::div(SOp::sub(hz0, hz_jm), a.dys);
         const double dHy_dz = SOp::div(SOp::sub(hy0, hyk), a.dzs);
@@ -267,78 +303,60 @@ __device__ __forceinline__ void d_update(const StepArgs<R>& a, int i, int j, int
         const double dHz_dx = SOp::div(SOp::sub(hz0, hz_im), a.dxs);
         const double dHy_dx = SOp::div(SOp::sub(hy0, hy_im), a.dxs);
         const double dHx_dy = SOp::div(SOp::sub(hx0, hx_jm), a.dys);
-        double pxy = 0.0, pxz = 0.0, pyx = 0.0, pyz = 0.0, pzx = 0.0, pzy = 0.0;
         double kappa_x = 1.0, kappa_y = 1.0, kappa_z = 1.0;
         if (sx >= 0) { /* fdtd.c:3258-3285 */
             kappa_x = ldg_nh(a.tx.kappa + i);
             const double b = ldg_nh(a.tx.b + i), cc = ldg_nh(a.tx.c + i);
             const int q = (k * a.ny + j) * L2 + sx;
-            pxy = a.psi.dxy[q];
-            pxz = a.psi.dxz[q];
-            a.psi.dxy[q] = SOp::add(SOp::mul(b, pxy), SOp::mul(cc, -dHz_dx));
-            a.psi.dxz[q] = SOp::add(SOp::mul(b, pxz), SOp::mul(cc, dHy_dx));
+            a.psi.dxy[q] = SOp::add(SOp::mul(b, ps.xy), SOp::mul(cc, -dHz_dx));
+            a.psi.dxz[q] = SOp::add(SOp::mul(b, ps.xz), SOp::mul(cc, dHy_dx));
         }
         if (sy >= 0) { /* fdtd.c:3288-3315 */
             kappa_y = ldg_nh(a.ty.kappa + j);
             const double b = ldg_nh(a.ty.b + j), cc = ldg_nh(a.ty.c + j);
             const int q = (k * L2 + sy) * a.nxp + i;
-            pyx = a.psi.dyx[q];
-            pyz = a.psi.dyz[q];
-            a.psi.dyx[q] = SOp::add(SOp::mul(b, pyx), SOp::mul(cc, dHz_dy));
-            a.psi.dyz[q] = SOp::add(SOp::mul(b, pyz), SOp::mul(cc, -dHx_dy));
+            a.psi.dyx[q] = SOp::add(SOp::mul(b, ps.yx), SOp::mul(cc, dHz_dy));
+            a.psi.dyz[q] = SOp::add(SOp::mul(b, ps.yz), SOp::mul(cc, -dHx_dy));
         }
-        int qz = 0;
-        if (sz >= 0) { /* fdtd.c:3318-3334 */
-            kappa_z = ldg_nh(a.tz.kappa + k);
-            qz = (sz * a.ny + j) * a.nxp + i;
-            pzx = a.psi.dzx[qz];
-            pzy = a.psi.dzy[qz];
-        }
+        if (sz >= 0) kappa_z = ldg_nh(a.tz.kappa + k); /* fdtd.c:3318-3334 */
         /* fdtd.c:3337-3339 */
-        const double ux = SOp::add(SOp::add(SOp::add(SOp::div(dHz_dy, kappa_y), pyx), SOp::div(-dHy_dz, kappa_z)), pzx);
-        const double uy = SOp::add(SOp::add(SOp::add(SOp::div(-dHz_dx, kappa_x), pxy), SOp::div(dHx_dz, kappa_z)), pzy);
-        const double uz = SOp::add(SOp::add(SOp::add(SOp::div(dHy_dx, kappa_x), pxz), SOp::div(-dHx_dy, kappa_y)), pyz);
+        const double ux = SOp::add(SOp::add(SOp::add(SOp::div(dHz_dy, kappa_y), ps.yx), SOp::div(-dHy_dz, kappa_z)), ps.zx);
+        const double uy = SOp::add(SOp::add(SOp::add(SOp::div(-dHz_dx, kappa_x), ps.xy), SOp::div(dHx_dz, kappa_z)), ps.zy);
+        const double uz = SOp::add(SOp::add(SOp::add(SOp::div(dHy_dx, kappa_x), ps.xz), SOp::div(-dHx_dy, kappa_y)), ps.yz);
         dx = SOp::add(dx, SOp::mul(a.dt, ux));
         dy = SOp::add(dy, SOp::mul(a.dt, uy));
         dz = SOp::add(dz, SOp::mul(a.dt, uz));
         if (sz >= 0) { /* fdtd.c:3340-3343 */
             const double b = ldg_nh(a.tz.b + k), cc = ldg_nh(a.tz.c + k);
-            a.psi.dzx[qz] = SOp::add(SOp::mul(b, pzx), SOp::mul(cc, -dHy_dz));
-            a.psi.dzy[qz] = SOp::add(SOp::mul(b, pzy), SOp::mul(cc, dHx_dz));
+            const int qz = (sz * a.ny + j) * a.nxp + i;
+            a.psi.dzx[qz] = SOp::add(SOp::mul(b, ps.zx), SOp::mul(cc, -dHy_dz));
+            a.psi.dzy[qz] = SOp::add(SOp::mul(b, ps.zy), SOp::mul(cc, dHx_dz));
         }
     } else {
         const R dHzy = hz0 - hz_jm, dHyz = hy0 - hyk, dHxz = hx0 - hxk;
         const R dHzx = hz0 - hz_im, dHyx = hy0 - hy_im, dHxy = hx0 - hx_jm;
         const R kdx = ldg(a.tx.kd + i), kdy = ldg(a.ty.kd + j), kdz = ldg_nh(a.tz.kd + k);
-        R ux = kdy * dHzy - kdz * dHyz;
-        R uy = -kdx * dHzx + kdz * dHxz;
-        R uz = kdx * dHyx - kdy * dHxy;
+        /* psi terms enter as zeros outside the PML */
+        R ux = kdy * dHzy - kdz * dHyz + ps.yx + ps.zx;
+        R uy = -kdx * dHzx + kdz * dHxz + ps.xy + ps.zy;
+        R uz = kdx * dHyx - kdy * dHxy + ps.xz + ps.yz;
         if (sx >= 0) {
             const R b = ldg_nh(a.tx.b + i), cd = ldg_nh(a.tx.cd + i);
             const int q = (k * a.ny + j) * L2 + sx;
-            const R pxy = a.psi.dxy[q], pxz = a.psi.dxz[q];
-            uy += pxy;
-            uz += pxz;
-            a.psi.dxy[q] = b * pxy - cd * dHzx;
-            a.psi.dxz[q] = b * pxz + cd * dHyx;
+            a.psi.dxy[q] = b * ps.xy - cd * dHzx;
+            a.psi.dxz[q] = b * ps.xz + cd * dHyx;
         }
         if (sy >= 0) {
             const R b = ldg_nh(a.ty.b + j), cd = ldg_nh(a.ty.cd + j);
             const int q = (k * L2 + sy) * a.nxp + i;
-            const R pyx = a.psi.dyx[q], pyz = a.psi.dyz[q];
-            ux += pyx;
-            uz += pyz;
-            a.psi.dyx[q] = b * pyx + cd * dHzy;
-            a.psi.dyz[q] = b * pyz - cd * dHxy;
+            a.psi.dyx[q] = b * ps.yx + cd * dHzy;
+            a.psi.dyz[q] = b * ps.yz - cd * dHxy;
         }
         if (sz >= 0) {
             const R b = ldg_nh(a.tz.b + k), cd = ldg_nh(a.tz.cd + k);
             const int q = (sz * a.ny + j) * a.nxp + i;
-            const R pzx = a.psi.dzx[q], pzy = a.psi.dzy[q];
-            ux += pzx;
-            uy += pzy;
-            a.psi.dzx[q] = b * pzx - cd * dHyz;
-            a.psi.dzy[q] = b * pzy + cd * dHxz;
+            a.psi.dzx[q] = b * ps.zx - cd * dHyz;
+            a.psi.dzy[q] = b * ps.zy + cd * dHxz;
         }
         dx += ux;
         dy += uy;
@@ -353,6 +371,15 @@ __device__ __forceinline__ void e_update(const StepArgs<R>& a, const MatCoef<R>&
                                          R dx, R dy, R dz, R& ex, R& ey, R& ez)
 {
     const int flags = m.flags;
+    if constexpr (!STRICT) {
+        if (flags & kIso) { /* vacuum and isotropic lossless dielectrics */
+            const R s = m.eps_inv[0];
+            ex = s * dx;
+            ey = s * dy;
+            ez = s * dz;
+            return;
+        }
+    }
     int64_t slot = -1;
     if (flags & (kAde | kAtoms)) slot = a.slot[c];
     const int64_t ns = a.nslot;
@@ -506,7 +533,7 @@ __device__ __forceinline__ void e_update(const StepArgs<R>& a, const MatCoef<R>&
 template <typename R, bool STRICT, int NAMAX>
 __device__ __forceinline__ void e_cell(const StepArgs<R>& a, int i, int j, int k, int c, bool interior, int sx, int sy,
                                        R hx0, R hy0, R hz0, R hxk, R hyk, R hz_jm, R hx_jm, R hz_im, R hy_im, R dx, R dy,
-                                       R dz, int mid)
+                                       R dz, int mid, const MatCoef<R>* mcs, const CellPsi<R>* pre)
 {
     R* __restrict__ dxp = a.f.dx;
     R* __restrict__ dyp = a.f.dy;
@@ -514,12 +541,16 @@ __device__ __forceinline__ void e_cell(const StepArgs<R>& a, int i, int j, int k
     R* __restrict__ exp_ = a.f.ex;
     R* __restrict__ eyp = a.f.ey;
     R* __restrict__ ezp = a.f.ez;
-    const MatCoef<R>& m = a.mc[mid];
+    /* mcs: the block's shared-memory copy of the first kSmemMats records */
+    const MatCoef<R>& m = (mcs && mid < a.nmat) ? mcs[mid] : a.mc[mid];
     const int flags = m.flags;
     R ex = R(0), ey = R(0), ez = R(0);
     if (flags & (kLossy | kAde)) { ex = exp_[c]; ey = eyp[c]; ez = ezp[c]; }
     if (interior) {
-        d_update<R, STRICT>(a, i, j, k, sx, sy, hx0, hy0, hz0, hxk, hyk, hz_jm, hx_jm, hz_im, hy_im, dx, dy, dz);
+        CellPsi<R> ps;
+        if (pre) ps = *pre;
+        else load_psi_d(a, i, j, k, sx, sy, ps);
+        d_update<R, STRICT>(a, i, j, k, sx, sy, hx0, hy0, hz0, hxk, hyk, hz_jm, hx_jm, hz_im, hy_im, ps, dx, dy, dz);
         if (flags & kLossy) { /* fdtd.c:3349-3353 */
             const R* q = m.eps_im;
             if constexpr (STRICT) {
@@ -623,7 +654,7 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : PHP_E_MINB
             hy_im = ldg(hy + c - 1);
         }
         e_cell<R, STRICT, NAMAX>(a, i, j, k, c, interior, sx, sy, cur.hx, cur.hy, cur.hz, hxk, hyk, hz_jm, hx_jm, hz_im,
-                                 hy_im, cur.dx, cur.dy, cur.dz, cur.mid);
+                                 hy_im, cur.dx, cur.dy, cur.dz, cur.mid, nullptr, nullptr);
         hxk = cur.hx;
         hyk = cur.hy;
 #if PHP_PREFETCH

@@ -34,6 +34,27 @@ namespace phpdev {
 constexpr int kTmaStages = 4;
 constexpr uint32_t kWaitLimit = 1u << 24;
 
+/* tuning: ring depth of the FP64 fused sweep, and whether the CPML state is
+ * read before the stage wait (1) or after it (0), per sweep and precision */
+#ifndef PHP_TMA_ES64
+#define PHP_TMA_ES64 3
+#endif
+#ifndef PHP_TMA_ES32
+#define PHP_TMA_ES32 4
+#endif
+#ifndef PHP_TMA_HS
+#define PHP_TMA_HS 4
+#endif
+#ifndef PHP_PSI_EARLY_H64
+#define PHP_PSI_EARLY_H64 1
+#endif
+#ifndef PHP_PSI_EARLY_H32
+#define PHP_PSI_EARLY_H32 0
+#endif
+#ifndef PHP_PSI_EARLY_E
+#define PHP_PSI_EARLY_E 1
+#endif
+
 /* Tensor maps of the device arrays (3-D: x, y, plane; planes count from the
  * low halo plane of the field arrays). */
 struct TmaMaps {
@@ -115,10 +136,16 @@ struct TmaGeom {
     static constexpr uint32_t H_STAGE = align128(3 * align128(HALO_BYTES) + 3 * align128(OWN_BYTES));
     /* E sweep stage: 3 halo H boxes + 3 own D boxes + material ids */
     static constexpr uint32_t E_STAGE = align128(3 * align128(HALO_BYTES) + 3 * align128(OWN_BYTES) + align128(MAT_BYTES));
+    /* ring depths: 4 planes, 3 for the FP64 fused sweep so that four
+     * blocks (with their material records) fit in one SM's shared memory */
+    static constexpr int HS = PHP_TMA_HS;
+    static constexpr int ES = sizeof(R) == 8 ? PHP_TMA_ES64 : PHP_TMA_ES32;
     /* dynamic shared memory: 128 bytes of alignment slack, the stages, then
      * the stage barriers */
-    static constexpr uint32_t H_SMEM = 128 + kTmaStages * H_STAGE + kTmaStages * 8;
-    static constexpr uint32_t E_SMEM = 128 + kTmaStages * E_STAGE + kTmaStages * 8;
+    static constexpr uint32_t H_SMEM = 128 + HS * H_STAGE + HS * 8;
+    /* the fused sweep adds its material records after 128 bytes of barriers:
+     * E_SMEM + nmat * sizeof(MatCoef<R>) */
+    static constexpr uint32_t E_SMEM = 128 + ES * E_STAGE + 128;
 };
 
 /* 128-byte aligned start of the stage ring inside dynamic shared memory */
@@ -138,7 +165,7 @@ __global__ void __launch_bounds__(kBlockX * kBlockY) h_sweep_tma(const __grid_co
     using G = TmaGeom<R>;
     extern __shared__ __align__(128) unsigned char dyn_smem[];
     unsigned char* smem = ring_base(dyn_smem);
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem + kTmaStages * G::H_STAGE);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + G::HS * G::H_STAGE);
 
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * G::TX + tx;
     const int i0 = blockIdx.x * G::TX, j0 = blockIdx.y * G::TY;
@@ -148,10 +175,10 @@ __global__ void __launch_bounds__(kBlockX * kBlockY) h_sweep_tma(const __grid_co
     if (k0 >= k1) return; /* uniform over the block */
 
     constexpr uint32_t EB = G::align128(G::HALO_BYTES), HB = G::align128(G::OWN_BYTES);
-    auto stage = [&](int p) -> unsigned char* { return smem + (uint32_t)((p - k0) % kTmaStages) * G::H_STAGE; };
+    auto stage = [&](int p) -> unsigned char* { return smem + (uint32_t)((p - k0) % G::HS) * G::H_STAGE; };
     /* plane p = k0..k1: E (halo boxes) of every plane, H of planes < k1 */
     auto issue = [&](int p) {
-        uint64_t* bar = &full[(p - k0) % kTmaStages];
+        uint64_t* bar = &full[(p - k0) % G::HS];
         unsigned char* b = stage(p);
         const bool with_h = p < k1;
         mbar_arrive_expect_tx(bar, 3 * G::HALO_BYTES + (with_h ? 3 * G::OWN_BYTES : 0u));
@@ -161,12 +188,12 @@ __global__ void __launch_bounds__(kBlockX * kBlockY) h_sweep_tma(const __grid_co
     };
 
     if (tid == 0) {
-        for (int s = 0; s < kTmaStages; ++s) mbar_init(&full[s], 1);
+        for (int s = 0; s < G::HS; ++s) mbar_init(&full[s], 1);
         fence_barrier_init();
     }
     __syncthreads();
     if (tid == 0)
-        for (int p = k0; p <= min(k1, k0 + kTmaStages - 1); ++p) issue(p);
+        for (int p = k0; p <= min(k1, k0 + G::HS - 1); ++p) issue(p);
 
     const bool active = (i < a.nx - 1) && (j < a.ny - 1);
     const int L2 = 2 * a.L;
@@ -187,9 +214,27 @@ __global__ void __launch_bounds__(kBlockX * kBlockY) h_sweep_tma(const __grid_co
     const int ho = ty * G::TX + tx; /* own cell in an own box */
 
     for (int k = k0; k < k1; ++k) {
+        /* CPML state and per-plane values do not depend on the staged planes:
+         * issue their loads first so their latency overlaps the wait */
+        constexpr bool early = sizeof(R) == 8 ? PHP_PSI_EARLY_H64 : PHP_PSI_EARLY_H32;
+        const int sz = ldg_nh(a.tz.slot + k);
+        R pxy = R(0), pxz = R(0), pyx = R(0), pyz = R(0), pzx = R(0), pzy = R(0);
+        const int qx = (k * ny + j) * L2 + sx, qy = (k * L2 + sy) * nxp + i, qz = (sz * ny + j) * nxp + i;
+        auto load_psi = [&]() {
+            if (active) {
+                if (sx >= 0) { pxy = a.psi.hxy[qx]; pxz = a.psi.hxz[qx]; }
+                if (sy >= 0) { pyx = a.psi.hyx[qy]; pyz = a.psi.hyz[qy]; }
+                if (sz >= 0) { pzx = a.psi.hzx[qz]; pzy = a.psi.hzy[qz]; }
+            }
+        };
+        if constexpr (early) load_psi();
+        R khz = R(0);
+        if constexpr (!STRICT) khz = ldg_nh(a.tz.kh + k);
+
         bool ok = true;
         if (k == k0) ok = mbar_wait(&full[0], 0);
-        ok = ok && mbar_wait(&full[(k + 1 - k0) % kTmaStages], ((k + 1 - k0) / kTmaStages) & 1);
+        ok = ok && mbar_wait(&full[(k + 1 - k0) % G::HS], ((k + 1 - k0) / G::HS) & 1);
+        if constexpr (!early) load_psi();
         if (ok && active) {
             const unsigned char* b0 = stage(k);
             const unsigned char* b1 = stage(k + 1);
@@ -207,7 +252,6 @@ __global__ void __launch_bounds__(kBlockX * kBlockY) h_sweep_tma(const __grid_co
             const R ezj = Ez0[eo + G::BX], exj = Ex0[eo + G::BX];
             const R hx0 = Hx0[ho], hy0 = Hy0[ho], hz0 = Hz0[ho];
             const int c = (k * ny + j) * nxp + i;
-            const int sz = ldg_nh(a.tz.slot + k);
             if constexpr (STRICT) {
                 const double mu0 = a.mu0;
                 /* fdtd.c:3132-3137 */
@@ -217,33 +261,20 @@ __global__ void __launch_bounds__(kBlockX * kBlockY) h_sweep_tma(const __grid_co
                 const double dEx_dz = SOp::div(SOp::sub(ex1, ex0), a.dzs);
                 const double dEx_dy = SOp::div(SOp::sub(exj, ex0), a.dys);
                 const double dEy_dx = SOp::div(SOp::sub(eyi, ey0), a.dxs);
-                double pxy = 0.0, pxz = 0.0, pyx = 0.0, pyz = 0.0, pzx = 0.0, pzy = 0.0;
                 double kappa_x = 1.0, kappa_y = 1.0, kappa_z = 1.0;
                 if (sx >= 0) { /* fdtd.c:3143-3170 */
                     kappa_x = ldg_nh(a.tx.kappa + i);
                     const double bb = ldg_nh(a.tx.b + i), cc = ldg_nh(a.tx.c + i);
-                    const int q = (k * ny + j) * L2 + sx;
-                    pxy = a.psi.hxy[q];
-                    pxz = a.psi.hxz[q];
-                    a.psi.hxy[q] = SOp::add(SOp::mul(bb, pxy), SOp::mul(cc, SOp::div(dEz_dx, mu0)));
-                    a.psi.hxz[q] = SOp::add(SOp::mul(bb, pxz), SOp::mul(cc, SOp::div(-dEy_dx, mu0)));
+                    a.psi.hxy[qx] = SOp::add(SOp::mul(bb, pxy), SOp::mul(cc, SOp::div(dEz_dx, mu0)));
+                    a.psi.hxz[qx] = SOp::add(SOp::mul(bb, pxz), SOp::mul(cc, SOp::div(-dEy_dx, mu0)));
                 }
                 if (sy >= 0) { /* fdtd.c:3173-3200 */
                     kappa_y = ldg_nh(a.ty.kappa + j);
                     const double bb = ldg_nh(a.ty.b + j), cc = ldg_nh(a.ty.c + j);
-                    const int q = (k * L2 + sy) * nxp + i;
-                    pyx = a.psi.hyx[q];
-                    pyz = a.psi.hyz[q];
-                    a.psi.hyx[q] = SOp::add(SOp::mul(bb, pyx), SOp::mul(cc, SOp::div(-dEz_dy, mu0)));
-                    a.psi.hyz[q] = SOp::add(SOp::mul(bb, pyz), SOp::mul(cc, SOp::div(dEx_dy, mu0)));
+                    a.psi.hyx[qy] = SOp::add(SOp::mul(bb, pyx), SOp::mul(cc, SOp::div(-dEz_dy, mu0)));
+                    a.psi.hyz[qy] = SOp::add(SOp::mul(bb, pyz), SOp::mul(cc, SOp::div(dEx_dy, mu0)));
                 }
-                int qz = 0;
-                if (sz >= 0) { /* fdtd.c:3203-3219 */
-                    kappa_z = ldg_nh(a.tz.kappa + k);
-                    qz = (sz * ny + j) * nxp + i;
-                    pzx = a.psi.hzx[qz];
-                    pzy = a.psi.hzy[qz];
-                }
+                if (sz >= 0) kappa_z = ldg_nh(a.tz.kappa + k); /* fdtd.c:3203-3219 */
                 /* fdtd.c:3222-3224 */
                 const double ux = SOp::add(SOp::add(SOp::add(SOp::div(SOp::div(-dEz_dy, mu0), kappa_y), pyx),
                                                     SOp::div(SOp::div(dEy_dz, mu0), kappa_z)), pzx);
@@ -262,40 +293,25 @@ __global__ void __launch_bounds__(kBlockX * kBlockY) h_sweep_tma(const __grid_co
             } else {
                 const R dEyz = ey1 - ey0, dEzy = ezj - ez0, dEzx = ezi - ez0;
                 const R dExz = ex1 - ex0, dExy = exj - ex0, dEyx = eyi - ey0;
-                const R khz = ldg_nh(a.tz.kh + k);
-                R ux = -khy * dEzy + khz * dEyz;
-                R uy = khx * dEzx - khz * dExz;
-                R uz = -khx * dEyx + khy * dExy;
+                /* psi terms enter as zeros outside the PML */
+                hxg[c] = hx0 + (-khy * dEzy + khz * dEyz + pyx + pzx);
+                hyg[c] = hy0 + (khx * dEzx - khz * dExz + pxy + pzy);
+                hzg[c] = hz0 + (-khx * dEyx + khy * dExy + pxz + pyz);
                 if (sx >= 0) {
                     const R bb = ldg_nh(a.tx.b + i), ch = ldg_nh(a.tx.ch + i);
-                    const int q = (k * ny + j) * L2 + sx;
-                    const R pxy = a.psi.hxy[q], pxz = a.psi.hxz[q];
-                    uy += pxy;
-                    uz += pxz;
-                    a.psi.hxy[q] = bb * pxy + ch * dEzx;
-                    a.psi.hxz[q] = bb * pxz - ch * dEyx;
+                    a.psi.hxy[qx] = bb * pxy + ch * dEzx;
+                    a.psi.hxz[qx] = bb * pxz - ch * dEyx;
                 }
                 if (sy >= 0) {
                     const R bb = ldg_nh(a.ty.b + j), ch = ldg_nh(a.ty.ch + j);
-                    const int q = (k * L2 + sy) * nxp + i;
-                    const R pyx = a.psi.hyx[q], pyz = a.psi.hyz[q];
-                    ux += pyx;
-                    uz += pyz;
-                    a.psi.hyx[q] = bb * pyx - ch * dEzy;
-                    a.psi.hyz[q] = bb * pyz + ch * dExy;
+                    a.psi.hyx[qy] = bb * pyx - ch * dEzy;
+                    a.psi.hyz[qy] = bb * pyz + ch * dExy;
                 }
                 if (sz >= 0) {
                     const R bb = ldg_nh(a.tz.b + k), ch = ldg_nh(a.tz.ch + k);
-                    const int q = (sz * ny + j) * nxp + i;
-                    const R pzx = a.psi.hzx[q], pzy = a.psi.hzy[q];
-                    ux += pzx;
-                    uy += pzy;
-                    a.psi.hzx[q] = bb * pzx + ch * dEyz;
-                    a.psi.hzy[q] = bb * pzy - ch * dExz;
+                    a.psi.hzx[qz] = bb * pzx + ch * dEyz;
+                    a.psi.hzy[qz] = bb * pzy - ch * dExz;
                 }
-                hxg[c] = hx0 + ux;
-                hyg[c] = hy0 + uy;
-                hzg[c] = hz0 + uz;
             }
         }
         /* every thread is done with plane k: its stage takes plane k + stages */
@@ -303,9 +319,9 @@ __global__ void __launch_bounds__(kBlockX * kBlockY) h_sweep_tma(const __grid_co
             if (tid == 0) atomicExch(a.err, 1);
             break;
         }
-        if (tid == 0 && k + kTmaStages <= k1) {
+        if (tid == 0 && k + G::HS <= k1) {
             fence_proxy_async_smem();
-            issue(k + kTmaStages);
+            issue(k + G::HS);
         }
     }
 }
@@ -321,7 +337,7 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : PHP_E_MINB
     using G = TmaGeom<R>;
     extern __shared__ __align__(128) unsigned char dyn_smem[];
     unsigned char* smem = ring_base(dyn_smem);
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem + kTmaStages * G::E_STAGE);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + G::ES * G::E_STAGE);
 
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * G::TX + tx;
     const int i0 = blockIdx.x * G::TX, j0 = blockIdx.y * G::TY;
@@ -332,9 +348,9 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : PHP_E_MINB
 
     constexpr uint32_t HB = G::align128(G::HALO_BYTES), OB = G::align128(G::OWN_BYTES);
     /* plane p = k0-1 .. k1-1 into stage (p - k0 + 1) % stages */
-    auto stage = [&](int p) -> unsigned char* { return smem + (uint32_t)((p - k0 + 1) % kTmaStages) * G::E_STAGE; };
+    auto stage = [&](int p) -> unsigned char* { return smem + (uint32_t)((p - k0 + 1) % G::ES) * G::E_STAGE; };
     auto issue = [&](int p) {
-        uint64_t* bar = &full[(p - k0 + 1) % kTmaStages];
+        uint64_t* bar = &full[(p - k0 + 1) % G::ES];
         unsigned char* b = stage(p);
         const bool own = p >= k0;
         mbar_arrive_expect_tx(bar, 3 * G::HALO_BYTES + (own ? 3 * G::OWN_BYTES + G::MAT_BYTES : 0u));
@@ -345,13 +361,21 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : PHP_E_MINB
         }
     };
 
+    /* material records of ids < a.nmat, copied after the barriers */
+    MatCoef<R>* mcs = reinterpret_cast<MatCoef<R>*>(smem + G::ES * G::E_STAGE + 128);
     if (tid == 0) {
-        for (int s = 0; s < kTmaStages; ++s) mbar_init(&full[s], 1);
+        for (int s = 0; s < G::ES; ++s) mbar_init(&full[s], 1);
         fence_barrier_init();
+    }
+    {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(a.mc);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(mcs);
+        const int words = a.nmat * (int)(sizeof(MatCoef<R>) / 4);
+        for (int t = tid; t < words; t += G::TX * G::TY) dst[t] = ldg(src + t);
     }
     __syncthreads();
     if (tid == 0)
-        for (int p = k0 - 1; p <= min(k1 - 1, k0 - 1 + kTmaStages - 1); ++p) issue(p);
+        for (int p = k0 - 1; p <= min(k1 - 1, k0 - 1 + G::ES - 1); ++p) issue(p);
 
     const bool active = (i < a.nx) && (j < a.ny);
     const bool interior = (i >= 1 && i < a.nx - 1 && j >= 1 && j < a.ny - 1);
@@ -361,9 +385,14 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : PHP_E_MINB
     const int oo = ty * G::TX + tx;                 /* own cell in an own box */
 
     for (int k = k0; k < k1; ++k) {
+        /* CPML state read before the wait (it does not depend on the stages) */
+        CellPsi<R> ps;
+        ps.sz = -1;
+        if (PHP_PSI_EARLY_E && active && interior) load_psi_d(a, i, j, k, sx, sy, ps);
         bool ok = true;
         if (k == k0) ok = mbar_wait(&full[0], 0);
-        ok = ok && mbar_wait(&full[(k - k0 + 1) % kTmaStages], ((k - k0 + 1) / kTmaStages) & 1);
+        ok = ok && mbar_wait(&full[(k - k0 + 1) % G::ES], ((k - k0 + 1) / G::ES) & 1);
+        if (!PHP_PSI_EARLY_E && active && interior) load_psi_d(a, i, j, k, sx, sy, ps);
         if (ok && active) {
             const unsigned char* bp = stage(k - 1);
             const unsigned char* bc = stage(k);
@@ -378,16 +407,17 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : PHP_E_MINB
             const uint8_t* M = reinterpret_cast<const uint8_t*>(bc + 3 * HB + 3 * OB);
             const int c = (k * a.ny + j) * a.nxp + i;
             e_cell<R, STRICT, NAMAX>(a, i, j, k, c, interior, sx, sy, Hx[ho], Hy[ho], Hz[ho], Hxp[ho], Hyp[ho],
-                                     Hz[ho - G::BX], Hx[ho - G::BX], Hz[ho - 1], Hy[ho - 1], Dx[oo], Dy[oo], Dz[oo], M[oo]);
+                                     Hz[ho - G::BX], Hx[ho - G::BX], Hz[ho - 1], Hy[ho - 1], Dx[oo], Dy[oo], Dz[oo], M[oo],
+                                     mcs, &ps);
         }
         /* every thread is done with plane k-1: its stage takes plane k-1 + stages */
         if (__syncthreads_or(!ok)) {
             if (tid == 0) atomicExch(a.err, 1);
             break;
         }
-        if (tid == 0 && k - 1 + kTmaStages <= k1 - 1) {
+        if (tid == 0 && k - 1 + G::ES <= k1 - 1) {
             fence_proxy_async_smem();
-            issue(k - 1 + kTmaStages);
+            issue(k - 1 + G::ES);
         }
     }
 }
