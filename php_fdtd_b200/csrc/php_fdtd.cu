@@ -86,7 +86,8 @@ struct php_ctx {
     size_t host_stage_bytes = 0;
 
     /* host copies kept for reads */
-    std::vector<int> mat_natom, mat_ade;
+    std::vector<int> mat_natom, mat_ade, mat_flags;
+    std::vector<double> mat_cs, mat_sn;
     std::vector<int32_t> slot_host_dummy;
 
     /* sources */
@@ -313,6 +314,22 @@ static MatCoef<R> pack_material(const php_ctx* ctx, const MatD& s, int ion_off)
         }
         o.gp_inv[q] = (R)s.gp_inv[q];
         o.gm[q] = (R)s.gm[q];
+    }
+    if (ctx->prec == PHP_PREC_FP32 && (s.flags & kAde)) {
+        /* increment form of the ADE recurrence (see e_update):
+         * A = (I + G)^-1 2G with G = I - gm, B = (I + G)^-1 eps0 dt^2 wp2,
+         * formed in double before rounding */
+        for (int r = 0; r < 3; r++)
+            for (int q = 0; q < 3; q++) {
+                double av = 0.0, bv = 0.0;
+                for (int t = 0; t < 3; t++) {
+                    const double g2 = 2.0 * ((t == q ? 1.0 : 0.0) - s.gm[t * 3 + q]); /* 2G[t][q] */
+                    av += s.gp_inv[r * 3 + t] * g2;
+                    bv += s.gp_inv[r * 3 + t] * s.wp2[t * 3 + q] * e0dt2;
+                }
+                o.gm[r * 3 + q] = (R)av;
+                o.wp2[r * 3 + q] = (R)bv;
+            }
     }
     o.lf = (R)s.lf;
     o.lt = (R)s.lt;
@@ -723,6 +740,9 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
         }
         ctx->mat_natom.push_back(mats[i].natom);
         ctx->mat_ade.push_back(mats[i].flags & kAde ? 1 : 0);
+        ctx->mat_flags.push_back(mats[i].flags);
+        ctx->mat_cs.push_back(mats[i].cs);
+        ctx->mat_sn.push_back(mats[i].sn);
     }
 
     /* medium census, slots, device material map */
@@ -858,15 +878,27 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
 
 /* ---------------------------------------------------------------- stepping */
 
-/* graph of n steps reading per-step input buffer b */
+static int record_graph(php_ctx* ctx, int n, int b, cudaGraphExec_t* out);
+
+/* graph of n steps reading per-step input buffer b; a new chunk length
+ * records the graphs of both buffers at once, so that a repeated step
+ * pattern instantiates nothing after its first pass */
 static int ensure_graph(php_ctx* ctx, int n, int b, cudaGraphExec_t* out)
 {
-    const int key = 2 * n + b;
-    auto it = ctx->graphs.find(key);
+    auto it = ctx->graphs.find(2 * n + b);
     if (it != ctx->graphs.end()) {
         *out = it->second;
         return PHP_OK;
     }
+    cudaGraphExec_t other;
+    int rc = record_graph(ctx, n, b ^ 1, &other);
+    if (rc) return rc;
+    return record_graph(ctx, n, b, out);
+}
+
+static int record_graph(php_ctx* ctx, int n, int b, cudaGraphExec_t* out)
+{
+    const int key = 2 * n + b;
     ctx->step_in = ctx->step_in_dev[b];
     step_fn fn = pick_step(ctx).launch;
     cudaGraph_t g = nullptr;
@@ -1132,9 +1164,41 @@ int php_read_cell_state(php_ctx* ctx, int32_t i, int32_t j, int32_t k, int32_t* 
         if (v) { int rc = fetch(ctx->v, q, &v[q]); if (rc) return rc; }
     }
     if (ctx->mat_ade[mid] && s >= 0) {
+        double pq[3], poq[3];
         for (int q = 0; q < 3; q++) {
-            if (p_ade) { int rc = fetch(ctx->P, q, &p_ade[q]); if (rc) return rc; }
-            if (p_ade_old) { int rc = fetch(ctx->Po, q, &p_ade_old[q]); if (rc) return rc; }
+            double p = 0.0, po = 0.0;
+            int rc = fetch(ctx->P, q, &p);
+            if (!rc) rc = fetch(ctx->Po, q, &po);
+            if (rc) return rc;
+            pq[q] = p;
+            poq[q] = po;
+        }
+        if (ctx->prec == PHP_PREC_FP32) {
+            /* FP32 keeps Q = D - P (lab frame) in the P pool and
+             * J = P - P_old (crystal frame) in the P_old pool */
+            double dl[3];
+            for (int q = 0; q < 3; q++) {
+                float dv = 0.f;
+                CK(cudaMemcpy(&dv, (const float*)ctx->f[3 + q] + c, sizeof(float), cudaMemcpyDeviceToHost));
+                dl[q] = (double)dv - pq[q];
+            }
+            const int fl = ctx->mat_flags[mid];
+            const double cs = ctx->mat_cs[mid], sn = ctx->mat_sn[mid];
+            if (fl & kRotZ) {
+                const double u = dl[0] * cs - dl[1] * sn, w = dl[0] * sn + dl[1] * cs;
+                dl[0] = u; dl[1] = w;
+            } else if (fl & kRotX) {
+                const double u = dl[1] * cs - dl[2] * sn, w = dl[1] * sn + dl[2] * cs;
+                dl[1] = u; dl[2] = w;
+            }
+            for (int q = 0; q < 3; q++) {
+                poq[q] = dl[q] - poq[q];
+                pq[q] = dl[q];
+            }
+        }
+        for (int q = 0; q < 3; q++) {
+            if (p_ade) p_ade[q] = pq[q];
+            if (p_ade_old) p_ade_old[q] = poq[q];
         }
     } else {
         for (int q = 0; q < 3; q++) {

@@ -365,10 +365,11 @@ __device__ __forceinline__ void d_update(const StepArgs<R>& a, int i, int j, int
 }
 
 /* D -> E, ADE and ions for one cell (fdtd.c:3404-3528).  ex..ez hold E^n on
- * entry (lab frame) and E^{n+1} on return; dx..dz are D^{n+1}. */
+ * entry (lab frame) and E^{n+1} on return; dx..dz are D^{n+1}; ix..iz are
+ * D^{n+1} - D^n as summed before rounding into D (FP32 only). */
 template <typename R, bool STRICT, int NAMAX>
 __device__ __forceinline__ void e_update(const StepArgs<R>& a, const MatCoef<R>& m, int c,
-                                         R dx, R dy, R dz, R& ex, R& ey, R& ez)
+                                         R dx, R dy, R dz, R ix, R iy, R iz, R& ex, R& ey, R& ez)
 {
     const int flags = m.flags;
     if constexpr (!STRICT) {
@@ -470,7 +471,7 @@ __device__ __forceinline__ void e_update(const StepArgs<R>& a, const MatCoef<R>&
             na = SOp::sub(na, SOp::mul(m.lt, na));
             nb = SOp::sub(nb, SOp::mul(m.lt, nb));
             nc = SOp::sub(nc, SOp::mul(m.lt, nc));
-        } else {
+        } else if constexpr (sizeof(R) == 8) {
             t0 = R(2) * p0 - (g[0] * o0 + g[1] * o1 + g[2] * o2) + (w[0] * ea + w[1] * eb + w[2] * ec);
             t1 = R(2) * p1 - (g[3] * o0 + g[4] * o1 + g[5] * o2) + (w[3] * ea + w[4] * eb + w[5] * ec);
             t2 = R(2) * p2 - (g[6] * o0 + g[7] * o1 + g[8] * o2) + (w[6] * ea + w[7] * eb + w[8] * ec);
@@ -482,6 +483,33 @@ __device__ __forceinline__ void e_update(const StepArgs<R>& a, const MatCoef<R>&
             na = (dav - n0) * m.ade_scale;
             nb = (dbv - n1) * m.ade_scale;
             nc = (dcv - n2) * m.ade_scale;
+        } else {
+            /* FP32: the same recurrence, rewritten so that no step cancels
+             * digits.  With J^n = P^n - P^{n-1},
+             *   J^{n+1} = J^n - A J^n + B E^n,  A = 2 (I + g dt/2)^-1 g dt/2,
+             *                                   B = (I + g dt/2)^-1 eps0 dt^2 wp2
+             * (A in gm, B in wp2), and E^{n+1} is taken from
+             * Q = D - P (lab frame), Q^{n+1} = Q^n + (D^{n+1} - D^n) - J^{n+1}
+             * in the crystal frame.  The pools hold Q (P pool) and J (P_old
+             * pool).  In a metal D and P agree to a few parts in 1e3, and
+             * 2 P^n - P^{n-1} to a few parts in 1e3 of P: both differences
+             * lose most single-precision digits and drift by percents over
+             * thousands of steps. */
+            (void)gi;
+            const R j0 = o0 - (g[0] * o0 + g[1] * o1 + g[2] * o2) + (w[0] * ea + w[1] * eb + w[2] * ec);
+            const R j1 = o1 - (g[3] * o0 + g[4] * o1 + g[5] * o2) + (w[3] * ea + w[4] * eb + w[5] * ec);
+            const R j2 = o2 - (g[6] * o0 + g[7] * o1 + g[8] * o2) + (w[6] * ea + w[7] * eb + w[8] * ec);
+            R qa = p0 + ix, qb = p1 + iy, qc = p2 + iz;
+            rot_fwd<STRICT>(flags, m.cs, m.sn, qa, qb, qc);
+            qa -= j0;
+            qb -= j1;
+            qc -= j2;
+            na = (qa - pr0) * m.ade_scale;
+            nb = (qb - pr1) * m.ade_scale;
+            nc = (qc - pr2) * m.ade_scale;
+            rot_back<STRICT>(flags, m.cs, m.sn, qa, qb, qc);
+            a.Po[slot] = j0; a.Po[ns + slot] = j1; a.Po[2 * ns + slot] = j2;
+            a.P[slot] = qa; a.P[ns + slot] = qb; a.P[2 * ns + slot] = qc;
         }
     }
 
@@ -546,11 +574,18 @@ __device__ __forceinline__ void e_cell(const StepArgs<R>& a, int i, int j, int k
     const int flags = m.flags;
     R ex = R(0), ey = R(0), ez = R(0);
     if (flags & (kLossy | kAde)) { ex = exp_[c]; ey = eyp[c]; ez = ezp[c]; }
+    /* FP32 sums this step's D increment on its own before adding it to D:
+     * the ADE update needs the increment without D's rounding */
+    constexpr bool kInc = !STRICT && sizeof(R) == 4;
+    R ix = R(0), iy = R(0), iz = R(0);
+    R& ux = kInc ? ix : dx;
+    R& uy = kInc ? iy : dy;
+    R& uz = kInc ? iz : dz;
     if (interior) {
         CellPsi<R> ps;
         if (pre) ps = *pre;
         else load_psi_d(a, i, j, k, sx, sy, ps);
-        d_update<R, STRICT>(a, i, j, k, sx, sy, hx0, hy0, hz0, hxk, hyk, hz_jm, hx_jm, hz_im, hy_im, ps, dx, dy, dz);
+        d_update<R, STRICT>(a, i, j, k, sx, sy, hx0, hy0, hz0, hxk, hyk, hz_jm, hx_jm, hz_im, hy_im, ps, ux, uy, uz);
         if (flags & kLossy) { /* fdtd.c:3349-3353 */
             const R* q = m.eps_im;
             if constexpr (STRICT) {
@@ -558,9 +593,9 @@ __device__ __forceinline__ void e_cell(const StepArgs<R>& a, int i, int j, int k
                 dy = SOp::sub(dy, SOp::mul(SOp::mul(a.c1, SOp::add(SOp::add(SOp::mul(q[3], ex), SOp::mul(q[4], ey)), SOp::mul(q[5], ez))), a.eps0));
                 dz = SOp::sub(dz, SOp::mul(SOp::mul(a.c1, SOp::add(SOp::add(SOp::mul(q[6], ex), SOp::mul(q[7], ey)), SOp::mul(q[8], ez))), a.eps0));
             } else {
-                dx -= q[0] * ex + q[1] * ey + q[2] * ez;
-                dy -= q[3] * ex + q[4] * ey + q[5] * ez;
-                dz -= q[6] * ex + q[7] * ey + q[8] * ez;
+                ux -= q[0] * ex + q[1] * ey + q[2] * ez;
+                uy -= q[3] * ex + q[4] * ey + q[5] * ez;
+                uz -= q[6] * ex + q[7] * ey + q[8] * ez;
             }
         }
     }
@@ -575,16 +610,21 @@ __device__ __forceinline__ void e_cell(const StepArgs<R>& a, int i, int j, int k
                 else if (a.src_comp[s] == 2) dz = SOp::add(dz, add);
             } else {
                 const R add = R(v * a.dt);
-                if (a.src_comp[s] == 0) dx += add;
-                else if (a.src_comp[s] == 1) dy += add;
-                else if (a.src_comp[s] == 2) dz += add;
+                if (a.src_comp[s] == 0) ux += add;
+                else if (a.src_comp[s] == 1) uy += add;
+                else if (a.src_comp[s] == 2) uz += add;
             }
         }
+    }
+    if constexpr (kInc) {
+        dx += ix;
+        dy += iy;
+        dz += iz;
     }
     dxp[c] = dx;
     dyp[c] = dy;
     dzp[c] = dz;
-    e_update<R, STRICT, NAMAX>(a, m, c, dx, dy, dz, ex, ey, ez);
+    e_update<R, STRICT, NAMAX>(a, m, c, dx, dy, dz, ix, iy, iz, ex, ey, ez);
     exp_[c] = ex;
     eyp[c] = ey;
     ezp[c] = ez;
