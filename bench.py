@@ -34,7 +34,7 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-WORKLOADS = {"cfg0": 0, "cfg1": 1, "cfg2": 2, "cfg4": 4}
+WORKLOADS = {"cfg0": 0, "cfg1": 1, "cfg2": 2, "cfg3": 3, "cfg4": 4}
 
 
 def parse():
@@ -52,6 +52,9 @@ def parse():
     p.add_argument("--acc-steps", type=int, default=None,
                    help="steps of the FP32-vs-FP64 error run (default: the configuration's tsteps; 0 = skip)")
     p.add_argument("--case-dir", default=None)
+    p.add_argument("--requests", type=int, default=256, help="cfg3: number of requests")
+    p.add_argument("--max-active", type=int, default=16, help="cfg3: simulations running at once")
+    p.add_argument("--baseline-sample", type=int, default=16, help="cfg3: requests run alone for the baselines")
     return p.parse_args()
 
 
@@ -420,6 +423,10 @@ def ref_sample_steps(V: int, k: int) -> int:
 def run_reference_arm(args, ws, rank):
     if rank != 0:
         return
+    if args.workload == "cfg3":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no serving mode (one simulation per "
+                          "mpirun); the serving line carries its sequential plain-FP64 baseline"}))
+        return
     case_dir = Path(args.case_dir or tempfile.gettempdir()) / f"php_bench_{args.workload}_{args.scale}_ref"
     case_dir.mkdir(parents=True, exist_ok=True)
     cfg_path = make_case(args.workload, args.scale, 10, case_dir)
@@ -459,11 +466,117 @@ def workload_name(args):
     return BASELINE_NAMES[WORKLOADS[args.workload]] + ("" if args.scale == 1.0 else f" (scale {args.scale})")
 
 
+def run_serving(args, ws, rank, local):
+    """cfg3: the request stream submitted at its Poisson arrival times to the
+    serving loop (FP32 mixed kernels, 150 GB budget); latency = completion
+    minus submission on the server clock.  Baseline: the same requests run
+    one after another with the plain FP64 path, timed on a sample and
+    extrapolated by cell-steps (a + b * cells * steps fitted on the sample)."""
+    from php_fdtd_b200 import Simulation
+    from php_fdtd_b200.serving import DftSpec, Server
+    from php_fdtd_b200.workloads import request_desc, serving_requests
+    reqs = serving_requests(args.requests, seed=rank)
+    built = [request_desc(r, "fp32", device=local) for r in reqs]  # host-side inputs, before the clock
+    cells = np.array([r["grid"][0] * r["grid"][1] * r["grid"][2] for r in reqs], dtype=np.float64)
+    steps = np.array([r["steps"] for r in reqs], dtype=np.float64)
+    sample = sorted(set(np.linspace(0, len(reqs) - 1, min(args.baseline_sample, len(reqs))).round().astype(int).tolist()))
+    served = {}
+    infos = {}
+    done_evt = threading.Event()
+    budget = 150 * 10 ** 9
+
+    with ClockSampler(local) as clocks, Server(memory_budget=budget, device=local, max_active=args.max_active) as srv:
+        def collector():
+            while len(infos) < len(reqs):
+                for info in srv.poll(timeout_ms=200):
+                    q = info["tag"]
+                    infos[q] = info
+                    if q in sample and info["status"] == 0:
+                        served[q] = srv.fetch_dft(info)
+                    else:
+                        srv.release(info["job"])
+            done_evt.set()
+        th = threading.Thread(target=collector, daemon=True)
+        th.start()
+        t0 = srv.clock()
+        for q, (r, (holder, dft)) in enumerate(zip(reqs, built)):
+            wait = t0 + r["arrival"] - srv.clock()
+            if wait > 0:
+                time.sleep(wait)
+            srv.submit(holder, r["steps"], DftSpec(dft["component"], dft["z_plane"], dft["freqs"]), tag=q)
+        done_evt.wait()
+        th.join()
+        stats = srv.stats()
+    bad = [i for i in infos.values() if i["status"] != 0]
+    lat = np.array([infos[q]["t_done"] - infos[q]["t_submit"] for q in range(len(reqs))])
+    queue_wait = np.array([infos[q]["t_admit"] - infos[q]["t_submit"] for q in range(len(reqs))])
+    t_first = min(i["t_submit"] for i in infos.values())
+    t_last = max(i["t_done"] for i in infos.values())
+    makespan = t_last - t_first
+    sims_h = len(reqs) / makespan * 3600.0
+
+    # baselines on the sample: plain FP64 alone (timed) and FP32 alone (identity check)
+    seq_t, err, same = [], [], 0
+    for q in sample:
+        h64, dft = request_desc(reqs[q], "fp64", device=local)
+        t1 = time.perf_counter()
+        with Simulation(h64) as sim:
+            pid = sim.dft_add(dft["component"], dft["z_plane"], dft["freqs"])
+            sim.step(reqs[q]["steps"])
+            f64 = sim.dft_read(pid)[0]
+        seq_t.append(time.perf_counter() - t1)
+        with Simulation(built[q][0]) as sim:
+            pid = sim.dft_add(dft["component"], dft["z_plane"], dft["freqs"])
+            sim.step(reqs[q]["steps"])
+            f32 = sim.dft_read(pid)[0]
+        if q in served:
+            same += int(np.array_equal(served[q], f32))
+            err.append(float(np.linalg.norm(served[q] - f64) / max(np.linalg.norm(f64), 1e-300)))
+    cs = cells * steps
+    A = np.vstack([np.ones(len(sample)), cs[sample]]).T
+    coef, *_ = np.linalg.lstsq(A, np.array(seq_t), rcond=None)
+    seq_total = float(np.sum(np.maximum(coef[0] + coef[1] * cs, 0.0)))
+    seq_sims_h = len(reqs) / seq_total * 3600.0
+    h2d = float(np.sum(cells) * 5 + np.sum(steps) * 8 * 4)
+    d2h = float(sum(16 * r["grid"][0] * r["grid"][1] for r in reqs))
+    line = {
+        "metric": "sims/h, serving loop (FP32 mixed, continuous batching)", "value": round(sims_h, 2), "unit": "sims/h",
+        "n_gpus": ws, "steps": int(steps.sum()), "warmup": 0, "ms_per_step": round(makespan / steps.sum() * 1e3, 6),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "impl": "ours",
+        "config": {"workload": "cfg3_serving_request stream", "requests": len(reqs), "arrivals": "Poisson 4/s",
+                   "edges": "log-uniform 64-192 per axis", "steps": "3000-12000", "pml": 8,
+                   "memory_budget_bytes": budget, "max_active": args.max_active, "chunk_steps": 256},
+        "latency_s": {"p50": round(float(np.percentile(lat, 50)), 3), "p95": round(float(np.percentile(lat, 95)), 3),
+                      "p99": round(float(np.percentile(lat, 99)), 3), "max": round(float(lat.max()), 3),
+                      "queue_wait_p50": round(float(np.percentile(queue_wait, 50)), 3)},
+        "makespan_s": round(makespan, 3), "gcell_updates_per_s": round(float(cs.sum()) / makespan / 1e9, 3),
+        "failed": len(bad), "server": stats,
+        "baseline_sequential_fp64": {"sims_per_h": round(seq_sims_h, 2), "sample": len(sample),
+                                     "fit_s": [float(coef[0]), float(coef[1])],
+                                     "speedup": round(sims_h / seq_sims_h, 3)},
+        "results": {"identical_to_alone": f"{same}/{len(served)}",
+                    "nearfield_rel_l2_vs_fp64_max": round(max(err), 9) if err else None,
+                    "target": 1e-3},
+        "e2e": {"value": round(sims_h, 2), "unit": "sims/h", "h2d_bytes_per_step": round(h2d / steps.sum(), 1),
+                "d2h_bytes_per_step": round(d2h / steps.sum(), 3),
+                "path": "php_batch_submit host descriptions -> php_batch_poll/fetch_dft, whole stream timed"},
+        "clocks": clocks.summary(),
+        "gpu_launches": int(steps.sum()) * 3,
+    }
+    if rank == 0:
+        print(json.dumps(line))
+
+
 def main():
     args = parse()
     ws, rank, local = dist_init()
     if args.impl == "reference":
         run_reference_arm(args, ws, rank)
+        barrier(ws)
+        return
+    if args.workload == "cfg3":
+        run_serving(args, ws, rank, local)
         barrier(ws)
         return
     sim, cfg, r = run_ours(args, ws, rank, local, args.precision)

@@ -156,6 +156,10 @@ const char* php_last_error(const php_ctx* ctx);
 int php_step(php_ctx* ctx, int32_t nsteps);
 int php_sync(php_ctx* ctx);
 int php_get_step(const php_ctx* ctx, int32_t* t);
+/* Records (without running) the CUDA graphs that php_step(ctx, nsteps) will
+ * launch, so that the first such call does not pay for their capture.
+ * Registering a probe or a DFT plane afterwards drops them again. */
+int php_prepare(php_ctx* ctx, int32_t nsteps);
 
 /* --- outputs -------------------------------------------------------------- */
 
@@ -217,6 +221,10 @@ int php_dft_read(php_ctx* ctx, int32_t id, double* out, int32_t* nsamples);
 
 /* Device bytes held by the context. */
 int php_memory_bytes(const php_ctx* ctx, uint64_t* bytes);
+/* Device bytes php_create would allocate for this description (before any
+ * php_dft_add / php_probe_set); needs no device.  Used for admission
+ * against a memory budget. */
+int php_estimate_bytes(const php_desc* desc, uint64_t* bytes);
 /* Number of kernel launches enqueued by the last php_step call. */
 int php_last_launch_count(const php_ctx* ctx, int32_t* launches);
 /* Stream the context enqueues on (a cudaStream_t), for event timing. */
@@ -224,11 +232,12 @@ int php_stream(const php_ctx* ctx, void** stream);
 
 /* Per-kernel timing.  While enabled, the recorded step graphs carry CUDA
  * events around every sweep kernel and php_step accumulates their device
- * time: ms[0] H sweep, ms[1] fused D/E sweep, ms[2] probe, ms[3] DFT, with
- * the number of launches of each in launches[0..3].  Enabling or disabling
- * resets the sums. */
+ * time: ms[0] H sweep, ms[1] fused D/E sweep, ms[2] probe, ms[3] DFT,
+ * ms[4] ion pass of many-atom cells, with the number of launches of each in
+ * launches[0..4] (both arrays hold 5 entries).  Enabling or disabling resets
+ * the sums. */
 int php_profile_enable(php_ctx* ctx, int32_t enable);
-int php_profile_read(php_ctx* ctx, double* ms4, int64_t* launches4);
+int php_profile_read(php_ctx* ctx, double* ms, int64_t* launches);
 
 /* --- allocation-free field maxima ------------------------------------------ */
 

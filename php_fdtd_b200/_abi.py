@@ -54,6 +54,28 @@ class Diag(C.Structure):
     _fields_ = [("max_e", _d), ("max_ex", _d), ("max_r", _d), ("argmax_r", _i * 5), ("pad_", _i)]
 
 
+class ServerDesc(C.Structure):
+    _fields_ = [("abi_version", _i), ("device", _i), ("memory_budget", C.c_uint64), ("max_active", _i),
+                ("chunk_steps", _i)]
+
+
+class DftRequest(C.Structure):
+    _fields_ = [("component", _i), ("z_plane", _i), ("first_step", _i), ("interval", _i), ("nfreq", _i),
+                ("cast_f32", _i), ("freq_hz", _dp)]
+
+
+class JobInfo(C.Structure):
+    _fields_ = [("job", C.c_int64), ("tag", C.c_uint64), ("status", _i), ("steps", _i), ("t_submit", _d),
+                ("t_admit", _d), ("t_done", _d), ("device_bytes", C.c_uint64), ("nx", _i), ("ny", _i), ("nfreq", _i),
+                ("dft_samples", _i), ("error", C.c_char * 256)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("queued", _i), ("running", _i), ("finished_unpolled", _i), ("peak_running", _i),
+                ("bytes_in_use", C.c_uint64), ("peak_bytes", C.c_uint64), ("submitted", C.c_int64),
+                ("completed", C.c_int64)]
+
+
 class HostMaterial(C.Structure):
     _fields_ = [("name", C.c_char * 64), ("eps_re", _d * 9), ("eps_im", _d * 9), ("sigma", _d), ("sigma_m", _d),
                 ("anglez", _d), ("anglex", _d), ("use_ade", _i), ("natom", _i), ("switchxz", _i),
@@ -98,6 +120,18 @@ DEVICE_SYMBOLS = {
     "php_stream": (_i, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "php_profile_enable": (_i, [C.c_void_p, _i]),
     "php_profile_read": (_i, [C.c_void_p, _dp, C.POINTER(C.c_int64)]),
+    "php_estimate_bytes": (_i, [C.POINTER(Desc), C.POINTER(C.c_uint64)]),
+    "php_prepare": (_i, [C.c_void_p, _i]),
+    "php_server_create": (_i, [C.POINTER(ServerDesc), C.POINTER(C.c_void_p)]),
+    "php_server_destroy": (_i, [C.c_void_p]),
+    "php_server_last_error": (C.c_char_p, [C.c_void_p]),
+    "php_server_clock": (_i, [C.c_void_p, _dp]),
+    "php_server_stats_read": (_i, [C.c_void_p, C.POINTER(ServerStats)]),
+    "php_batch_submit": (_i, [C.c_void_p, C.POINTER(Desc), _i, C.POINTER(DftRequest), C.c_uint64,
+                              C.POINTER(C.c_int64)]),
+    "php_batch_poll": (_i, [C.c_void_p, C.POINTER(JobInfo), _i, _i, C.POINTER(_i)]),
+    "php_batch_fetch_dft": (_i, [C.c_void_p, C.c_int64, _dp]),
+    "php_batch_release": (_i, [C.c_void_p, C.c_int64]),
 }
 
 HOST_SYMBOLS = {
@@ -114,6 +148,8 @@ HOST_SYMBOLS = {
 }
 
 _STRUCTS = {"php_desc": Desc, "php_material_desc": MaterialDesc, "php_source_desc": SourceDesc, "php_diag": Diag,
+            "php_server_desc": ServerDesc, "php_dft_request": DftRequest, "php_job_info": JobInfo,
+            "php_server_stats": ServerStats,
             "php_cfg": Cfg, "php_host_material": HostMaterial}
 
 _host = None

@@ -64,7 +64,7 @@ def build_host(verbose: bool = False) -> Path:
 
 def build_device(verbose: bool = False) -> Path:
     out = PKG / "libphpfdtd.so"
-    sources = [CSRC / "php_fdtd.cu", CSRC / "php_noalloc.cu"]
+    sources = [CSRC / "php_fdtd.cu", CSRC / "php_noalloc.cu", CSRC / "php_serve.cu"]
     deps = sources + [INC / "php_fdtd.h"] + [p for p in CSRC.glob("*.cuh")]
     if _stale(out, deps):
         _run([_nvcc(), *NVCC_ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",

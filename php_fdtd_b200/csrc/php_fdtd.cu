@@ -23,6 +23,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -31,10 +32,11 @@ using namespace phpdev;
 namespace {
 
 constexpr int kMaxChunk = 256;      /* steps per recorded graph */
+constexpr int kProfKinds = 5;       /* H sweep, E sweep, probe, DFT, ion pass */
 constexpr int kProbeCap = 8192;     /* probe rows held on the device */
 constexpr double kEpsInf = 20.0;    /* EPS_INF, fdtd.c:202 */
 
-std::string g_create_error;
+thread_local std::string g_create_error; /* errors of php_create, per calling thread */
 
 struct DftPlane {
     int comp, z, first, interval, nfreq, cast_f32;
@@ -118,9 +120,16 @@ struct php_ctx {
 
     /* per-kernel timing (php_profile_enable) */
     bool profile = false;
-    std::vector<cudaEvent_t> prof_ev;   /* [kMaxChunk][4 kinds][begin, end] */
-    double prof_ms[4] = {};
-    int64_t prof_n[4] = {};
+    std::vector<cudaEvent_t> prof_ev;   /* [kMaxChunk][kProfKinds][begin, end] */
+    double prof_ms[kProfKinds] = {};
+    int64_t prof_n[kProfKinds] = {};
+
+    /* many-atom cells: ion pass apart from the E sweep (php_ions.cuh) */
+    bool ion_split = false, ion_tc = false;
+    int ion_np = 0;              /* 3N padded to 16 */
+    void* Pr = nullptr;          /* [3][nslot] */
+    void* ion_dmm = nullptr;     /* CUDA-core kernel: [np][np] R */
+    void* ion_bsplit = nullptr;  /* tensor kernel: DMM hi, lo bf16 images */
 };
 
 /* ------------------------------------------------------------------ utils */
@@ -145,14 +154,19 @@ static int fail(php_ctx* c, int code, const char* fmt, ...)
                         __FILE__, __LINE__);                                                       \
     } while (0)
 
+/* Device buffers come from the device's stream-ordered pool, allocated and
+ * freed on the context's stream: destroying one context never waits for the
+ * work of the others (cudaFree would synchronise the whole device), which
+ * the serving loop relies on. */
 static int dalloc(php_ctx* ctx, void** p, size_t bytes)
 {
     *p = nullptr;
     if (bytes == 0) bytes = 16;
-    cudaError_t e = cudaMalloc(p, bytes);
+    cudaError_t e = cudaMallocAsync(p, bytes, ctx->stream);
     if (e != cudaSuccess) {
         *p = nullptr;
-        return fail(ctx, PHP_ERR_OOM, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+        cudaGetLastError();
+        return fail(ctx, PHP_ERR_OOM, "cudaMallocAsync(%zu) failed: %s", bytes, cudaGetErrorString(e));
     }
     ctx->allocs.push_back(*p);
     ctx->bytes += bytes;
@@ -460,6 +474,7 @@ static StepArgs<R> make_args(php_ctx* ctx, int s_local)
     a.Po = (R*)ctx->Po;
     a.r = (R*)ctx->r;
     a.v = (R*)ctx->v;
+    a.pr = ctx->ion_split ? (const R*)ctx->Pr : nullptr;
     a.nslot = ctx->nslot;
 #ifndef PHP_SMEM_MATS
 #define PHP_SMEM_MATS 0
@@ -494,7 +509,50 @@ static StepArgs<R> make_args(php_ctx* ctx, int s_local)
 static inline void prof_mark(php_ctx* ctx, int s_local, int kind, int end)
 {
     if (ctx->profile)
-        cudaEventRecordWithFlags(ctx->prof_ev[((size_t)s_local * 4 + kind) * 2 + end], ctx->stream, cudaEventRecordExternal);
+        cudaEventRecordWithFlags(ctx->prof_ev[((size_t)s_local * kProfKinds + kind) * 2 + end], ctx->stream,
+                                 cudaEventRecordExternal);
+}
+
+template <typename R>
+static void launch_ions(php_ctx* ctx)
+{
+    IonArgs<R> a;
+    memset(&a, 0, sizeof(a));
+    R* const* fp = reinterpret_cast<R* const*>(ctx->f);
+    a.ex = fp[0];
+    a.ey = fp[1];
+    a.ez = fp[2];
+    a.r = (R*)ctx->r;
+    a.v = (R*)ctx->v;
+    a.pr = (R*)ctx->Pr;
+    a.slot_cell = ctx->slot_cell;
+    a.slot_n3 = ctx->slot_n3;
+    a.mat = ctx->mat;
+    a.mc = (const MatCoef<R>*)ctx->mc;
+    a.ion_coef = (const R*)ctx->ion_coef;
+    a.dmm = (const R*)ctx->ion_dmm;
+    a.bsplit = (const uint32_t*)ctx->ion_bsplit;
+    a.nslot = ctx->nslot;
+    a.ntiles = (int32_t)((ctx->nslot + kIonTile - 1) / kIonTile);
+    a.dt = ctx->d.dt;
+    a.err = ctx->err_flag;
+    const int grid = (int)std::min<int64_t>(a.ntiles, 148 * 4);
+    cudaStream_t st = ctx->stream;
+    if constexpr (sizeof(R) == 4) {
+        switch (ctx->ion_np) {
+        case 16: ion_update_tc<16><<<grid, kIonTile, IonTc<16>::SMEM, st>>>(a); break;
+        case 32: ion_update_tc<32><<<grid, kIonTile, IonTc<32>::SMEM, st>>>(a); break;
+        case 48: ion_update_tc<48><<<grid, kIonTile, IonTc<48>::SMEM, st>>>(a); break;
+        default: ion_update_tc<64><<<grid, kIonTile, IonTc<64>::SMEM, st>>>(a); break;
+        }
+    } else {
+        switch (ctx->ion_np) {
+        case 16: ion_update_cc<R, 16><<<grid, kIonTile, 0, st>>>(a); break;
+        case 32: ion_update_cc<R, 32><<<grid, kIonTile, 0, st>>>(a); break;
+        case 48: ion_update_cc<R, 48><<<grid, kIonTile, 0, st>>>(a); break;
+        default: ion_update_cc<R, 64><<<grid, kIonTile, 0, st>>>(a); break;
+        }
+    }
 }
 
 template <typename R, bool STRICT, int NA>
@@ -513,6 +571,14 @@ static void launch_step_t(php_ctx* ctx, int s_local, int& launches)
     else e_sweep<R, STRICT, NA><<<grid, block, 0, ctx->stream>>>(a);
     prof_mark(ctx, s_local, 1, 1);
     launches += 2;
+    if constexpr (!STRICT && NA == 0) {
+        if (ctx->ion_split) {
+            prof_mark(ctx, s_local, 4, 0);
+            launch_ions<R>(ctx);
+            prof_mark(ctx, s_local, 4, 1);
+            launches++;
+        }
+    }
     if (ctx->probe) {
         prof_mark(ctx, s_local, 2, 0);
         R* const* fp = reinterpret_cast<R* const*>(ctx->f);
@@ -573,9 +639,11 @@ static StepKernels pick_na(int namax)
 
 static StepKernels pick_step(const php_ctx* ctx)
 {
+    /* with the ion pass apart, the E sweep carries no per-atom state */
+    const int na = ctx->ion_split ? 0 : ctx->namax_tpl;
     if (ctx->prec == PHP_PREC_FP64_STRICT) return pick_na<double, true>(ctx->namax_tpl);
-    if (ctx->prec == PHP_PREC_FP64) return pick_na<double, false>(ctx->namax_tpl);
-    return pick_na<float, false>(ctx->namax_tpl);
+    if (ctx->prec == PHP_PREC_FP64) return pick_na<double, false>(na);
+    return pick_na<float, false>(na);
 }
 
 /* ------------------------------------------------------------ tensor maps */
@@ -658,19 +726,54 @@ static int upload_tables(php_ctx* ctx, const std::vector<MatD>& mats, const std:
     return PHP_OK;
 }
 
+/* Page-locked host buffers, kept for reuse by later contexts: freeing one
+ * (cudaFreeHost) can wait for the whole device, which would stall the other
+ * contexts a serving loop runs beside it. */
+static std::mutex g_pinned_mu;
+static std::multimap<size_t, void*> g_pinned_free;
+static std::map<void*, size_t> g_pinned_size;
+
+static void* pinned_get(size_t bytes)
+{
+    {
+        std::lock_guard<std::mutex> g(g_pinned_mu);
+        auto it = g_pinned_free.lower_bound(bytes);
+        if (it != g_pinned_free.end() && it->first <= 2 * bytes) {
+            void* p = it->second;
+            g_pinned_free.erase(it);
+            return p;
+        }
+    }
+    void* p = nullptr;
+    if (cudaMallocHost(&p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> g(g_pinned_mu);
+    g_pinned_size[p] = bytes;
+    return p;
+}
+
+static void pinned_put(void* p)
+{
+    if (!p) return;
+    std::lock_guard<std::mutex> g(g_pinned_mu);
+    g_pinned_free.emplace(g_pinned_size[p], p);
+}
+
 static void ctx_free(php_ctx* ctx)
 {
     if (!ctx) return;
     for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.second);
     ctx->graphs.clear();
-    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    for (void* p : ctx->allocs) cudaFree(p);
+    for (void* p : ctx->allocs) cudaFreeAsync(p, ctx->stream);
     ctx->allocs.clear();
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (cudaEvent_t e : ctx->prof_ev) cudaEventDestroy(e);
     ctx->prof_ev.clear();
-    if (ctx->host_stage) cudaFreeHost(ctx->host_stage);
+    pinned_put(ctx->host_stage);
     for (int b = 0; b < 2; ++b) {
-        if (ctx->step_in_host[b]) cudaFreeHost(ctx->step_in_host[b]);
+        pinned_put(ctx->step_in_host[b]);
         if (ctx->staged[b]) cudaEventDestroy(ctx->staged[b]);
     }
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -686,12 +789,87 @@ static int alloc_step_inputs(php_ctx* ctx, int row)
     for (int b = 0; b < 2; ++b) {
         int rc = dalloc(ctx, (void**)&ctx->step_in_dev[b], (size_t)kMaxChunk * row * sizeof(double));
         if (rc) return rc;
-        if (ctx->step_in_host[b]) cudaFreeHost(ctx->step_in_host[b]);
-        ctx->step_in_host[b] = nullptr;
-        CK(cudaMallocHost((void**)&ctx->step_in_host[b], (size_t)kMaxChunk * row * sizeof(double)));
+        pinned_put(ctx->step_in_host[b]);
+        ctx->step_in_host[b] = (double*)pinned_get((size_t)kMaxChunk * row * sizeof(double));
+        if (!ctx->step_in_host[b]) return fail(ctx, PHP_ERR_OOM, "page-locked host allocation failed");
         if (!ctx->staged[b]) CK(cudaEventCreateWithFlags(&ctx->staged[b], cudaEventDisableTiming));
     }
     ctx->step_in = ctx->step_in_dev[0];
+    return PHP_OK;
+}
+
+/* bf16 bits of x, rounded to nearest even (finite inputs) */
+static uint16_t bf16_bits(float x)
+{
+    uint32_t u;
+    memcpy(&u, &x, 4);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
+
+static double bf16_value(uint16_t b)
+{
+    const uint32_t u = (uint32_t)b << 16;
+    float f;
+    memcpy(&f, &u, 4);
+    return (double)f;
+}
+
+/* Many-atom cells (3N >= 24, one DMM shared by every atom material) get the
+ * ion pass of php_ions.cuh in the fast FP64 and FP32 paths; PHP_IONS=fused
+ * keeps the update inside the E sweep (for A/B timing). */
+static int setup_ion_pass(php_ctx* ctx, const std::vector<MatD>& mats, const php_desc& d)
+{
+    const char* iv = getenv("PHP_IONS");
+    if ((iv && !strcmp(iv, "fused")) || ctx->prec == PHP_PREC_FP64_STRICT || ctx->n3max < 24 || ctx->n3max > 64)
+        return PHP_OK;
+    int ref = -1;
+    for (int i = 0; i < d.num_materials; i++) {
+        if (mats[i].natom == 0) continue;
+        if (ref < 0) {
+            ref = i;
+            continue;
+        }
+        const int N = mats[i].natom;
+        if (N != mats[ref].natom || memcmp(d.materials[i].dmm, d.materials[ref].dmm, sizeof(double) * 9 * N * N))
+            return PHP_OK; /* several lattices: keep the fused update */
+    }
+    if (ref < 0) return PHP_OK;
+    const int n3 = 3 * mats[ref].natom, np = (n3 + 15) / 16 * 16;
+    const double* D = d.materials[ref].dmm;
+    const size_t rs = rsize(ctx->prec);
+    int rc = dalloc(ctx, &ctx->Pr, 3 * (size_t)ctx->nslot * rs);
+    if (rc) return rc;
+    if (ctx->prec == PHP_PREC_FP32) {
+        /* B operand of D = r DMM^T: row n = output coordinate q, k = p */
+        std::vector<uint16_t> img(2 * (size_t)np * np, 0);
+        for (int q = 0; q < n3; q++)
+            for (int p = 0; p < n3; p++) {
+                const double x = D[(size_t)q * n3 + p];
+                const uint16_t hi = bf16_bits((float)x);
+                const uint16_t lo = bf16_bits((float)(x - bf16_value(hi)));
+                const size_t off = umma_kmajor_off(q, p, np) / 2;
+                img[off] = hi;
+                img[(size_t)np * np + off] = lo;
+            }
+        if ((rc = dalloc(ctx, &ctx->ion_bsplit, img.size() * 2))) return rc;
+        CK(cudaMemcpyAsync(ctx->ion_bsplit, img.data(), img.size() * 2, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        cudaError_t e = cudaSuccess;
+        if (np == 64)
+            e = cudaFuncSetAttribute(ion_update_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)IonTc<64>::SMEM);
+        if (e != cudaSuccess) return fail(ctx, PHP_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+        ctx->ion_tc = true;
+    } else {
+        std::vector<double> pad((size_t)np * np, 0.0);
+        for (int q = 0; q < n3; q++)
+            for (int p = 0; p < n3; p++) pad[(size_t)q * np + p] = D[(size_t)q * n3 + p];
+        if ((rc = dalloc(ctx, &ctx->ion_dmm, pad.size() * sizeof(double)))) return rc;
+        CK(cudaMemcpyAsync(ctx->ion_dmm, pad.data(), pad.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    ctx->ion_np = np;
+    ctx->ion_split = true;
     return PHP_OK;
 }
 
@@ -845,6 +1023,7 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
         if ((rc = dalloc(ctx, &ctx->r, (size_t)n3max * ctx->nslot * rs))) return rc;
         if ((rc = dalloc(ctx, &ctx->v, (size_t)n3max * ctx->nslot * rs))) return rc;
     }
+    if ((rc = setup_ion_pass(ctx, mats, d))) return rc;
 
     AxisD axes[3];
     derive_axis(d, nx, d.dx, false, axes[0]);
@@ -871,8 +1050,55 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
     ctx->scratch_bytes = std::max(maxplane * sizeof(double), (size_t)4096 * sizeof(DiagPartial));
     if ((rc = dalloc(ctx, &ctx->scratch, ctx->scratch_bytes))) return rc;
     ctx->host_stage_bytes = ctx->scratch_bytes;
-    CK(cudaMallocHost(&ctx->host_stage, ctx->host_stage_bytes));
+    ctx->host_stage = pinned_get(ctx->host_stage_bytes);
+    if (!ctx->host_stage) return fail(ctx, PHP_ERR_OOM, "page-locked host allocation failed");
     CK(cudaStreamSynchronize(ctx->stream));
+    return PHP_OK;
+}
+
+/* Device bytes php_create will allocate for a description (the buffers of
+ * create_impl, without DFT planes or the probe ring); no device needed. */
+static int estimate_bytes(const php_desc& d, uint64_t* out)
+{
+    if (d.nx < 2 || d.ny < 2 || d.nz < 1 || d.num_materials < 1 || !d.materials || !d.medium || d.pml_thickness < 0 ||
+        d.precision < 0 || d.precision > 2)
+        return PHP_ERR_INPUT;
+    const uint64_t rs = d.precision == PHP_PREC_FP32 ? 4 : 8;
+    const uint64_t nxp = (uint64_t)(d.nx + 31) / 32 * 32, plane = nxp * d.ny, ncell = plane * d.nz;
+    std::vector<int> n3(d.num_materials, 0);
+    std::vector<char> slotted(d.num_materials, 0);
+    bool any_ade = false, any_atoms = false;
+    for (int m = 0; m < d.num_materials; m++) {
+        n3[m] = 3 * std::max(0, (int)d.materials[m].natom);
+        slotted[m] = d.materials[m].use_ade == 1 || d.materials[m].natom > 0;
+    }
+    uint64_t nslot = 0;
+    int n3max = 0;
+    const size_t V = (size_t)d.nx * d.ny * d.nz;
+    for (size_t c = 0; c < V; c++) {
+        const int id = d.medium[c];
+        if (id < 0 || id >= d.num_materials) return PHP_ERR_INPUT;
+        if (slotted[id]) {
+            nslot++;
+            n3max = std::max(n3max, n3[id]);
+            if (d.materials[id].use_ade == 1) any_ade = true;
+            if (d.materials[id].natom > 0) any_atoms = true;
+        }
+    }
+    const uint64_t L = d.pml_thickness;
+    uint64_t b = 9 * plane * (d.nz + 2) * rs;
+    b += 4 * ((uint64_t)d.nz * d.ny * 2 * L + (uint64_t)d.nz * 2 * L * nxp + 2 * L * d.ny * nxp) * rs;
+    b += ncell; /* material ids */
+    if (nslot) b += ncell * 4 + nslot * 12;
+    if (any_ade) b += 6 * nslot * rs;
+    if (any_atoms) b += 2 * (uint64_t)n3max * nslot * rs;
+    if (n3max >= 24 && d.precision != PHP_PREC_FP64_STRICT) b += 3 * nslot * rs + 64 * 64 * 8; /* ion pass */
+    b += 7 * (uint64_t)(d.nx + d.ny + d.nz) * (rs + 4);
+    b += 2 * (uint64_t)kMaxChunk * (std::max(1, (int)d.num_sources) + 8) * 8;
+    b += std::max((uint64_t)std::max({(uint64_t)d.nx * d.ny, (uint64_t)d.ny * d.nz, (uint64_t)d.nx * d.nz}) * 8,
+                  (uint64_t)4096 * sizeof(DiagPartial));
+    b += (uint64_t)d.num_materials * 512 + (1u << 20); /* tables, pool granularity */
+    *out = b;
     return PHP_OK;
 }
 
@@ -1024,18 +1250,33 @@ int php_step(php_ctx* ctx, int32_t nsteps)
         if (ctx->profile) {
             CK(cudaStreamSynchronize(ctx->stream));
             for (int s = 0; s < n; s++)
-                for (int kind = 0; kind < 4; kind++) {
-                    if ((kind == 2 && !ctx->probe) || (kind == 3 && ctx->dft.empty())) continue;
+                for (int kind = 0; kind < kProfKinds; kind++) {
+                    if ((kind == 2 && !ctx->probe) || (kind == 3 && ctx->dft.empty()) || (kind == 4 && !ctx->ion_split))
+                        continue;
                     float ms = 0.f;
-                    CK(cudaEventElapsedTime(&ms, ctx->prof_ev[((size_t)s * 4 + kind) * 2], ctx->prof_ev[((size_t)s * 4 + kind) * 2 + 1]));
+                    CK(cudaEventElapsedTime(&ms, ctx->prof_ev[((size_t)s * kProfKinds + kind) * 2],
+                                            ctx->prof_ev[((size_t)s * kProfKinds + kind) * 2 + 1]));
                     ctx->prof_ms[kind] += ms;
                     ctx->prof_n[kind] += kind == 3 ? (int64_t)ctx->dft.size() : 1;
                 }
         }
-        ctx->last_launches += n * (2 + (ctx->probe ? 1 : 0) + (int)ctx->dft.size());
+        ctx->last_launches += n * (2 + (ctx->ion_split ? 1 : 0) + (ctx->probe ? 1 : 0) + (int)ctx->dft.size());
         ctx->t += n;
         nsteps -= n;
     }
+    return PHP_OK;
+}
+
+int php_prepare(php_ctx* ctx, int32_t nsteps)
+{
+    if (!ctx) return PHP_ERR_INPUT;
+    if (nsteps < 0) return fail(ctx, PHP_ERR_INPUT, "negative step count");
+    cudaGraphExec_t g;
+    if (nsteps >= kMaxChunk) {
+        int rc = ensure_graph(ctx, kMaxChunk, 0, &g);
+        if (rc) return rc;
+    }
+    if (nsteps % kMaxChunk) return ensure_graph(ctx, nsteps % kMaxChunk, 0, &g);
     return PHP_OK;
 }
 
@@ -1341,6 +1582,12 @@ int php_memory_bytes(const php_ctx* ctx, uint64_t* bytes)
     return PHP_OK;
 }
 
+int php_estimate_bytes(const php_desc* desc, uint64_t* bytes)
+{
+    if (!desc || !bytes) return PHP_ERR_INPUT;
+    return estimate_bytes(*desc, bytes);
+}
+
 int php_last_launch_count(const php_ctx* ctx, int32_t* launches)
 {
     if (!ctx || !launches) return PHP_ERR_INPUT;
@@ -1360,24 +1607,24 @@ int php_profile_enable(php_ctx* ctx, int32_t enable)
     if (!ctx) return PHP_ERR_INPUT;
     drop_graphs(ctx);
     if (enable && ctx->prof_ev.empty()) {
-        ctx->prof_ev.resize((size_t)kMaxChunk * 4 * 2);
+        ctx->prof_ev.resize((size_t)kMaxChunk * kProfKinds * 2);
         for (auto& e : ctx->prof_ev) CK(cudaEventCreate(&e));
     }
     ctx->profile = enable != 0;
-    for (int q = 0; q < 4; q++) {
+    for (int q = 0; q < kProfKinds; q++) {
         ctx->prof_ms[q] = 0.0;
         ctx->prof_n[q] = 0;
     }
     return PHP_OK;
 }
 
-int php_profile_read(php_ctx* ctx, double* ms4, int64_t* launches4)
+int php_profile_read(php_ctx* ctx, double* ms, int64_t* launches)
 {
     if (!ctx) return PHP_ERR_INPUT;
     CK(cudaStreamSynchronize(ctx->stream));
-    for (int q = 0; q < 4; q++) {
-        if (ms4) ms4[q] = ctx->prof_ms[q];
-        if (launches4) launches4[q] = ctx->prof_n[q];
+    for (int q = 0; q < kProfKinds; q++) {
+        if (ms) ms[q] = ctx->prof_ms[q];
+        if (launches) launches[q] = ctx->prof_n[q];
     }
     return PHP_OK;
 }

@@ -100,6 +100,7 @@ struct StepArgs {
     const MatCoef<R>* mc;
     const R* ion_coef;
     R *P, *Po, *r, *v;         /* pools */
+    const R* pr;               /* QeZV . r [3][nslot] when the ion pass runs apart (php_ions.cuh), else null */
     int64_t nslot;
     int32_t nmat;
     int32_t nx, ny, nz, nxp, L, zchunk;
@@ -334,3 +335,4 @@ __global__ void __launch_bounds__(256) diag_pass2(const DiagPartial* scratch, in
 
 #include "php_sweeps.cuh"
 #include "php_sweeps_tma.cuh"
+#include "php_ions.cuh"

@@ -413,6 +413,15 @@ __device__ __forceinline__ void e_update(const StepArgs<R>& a, const MatCoef<R>&
         }
     }
 
+    if constexpr (!STRICT && NAMAX == 0) {
+        /* many-atom cells: P_ion = QeZV . r^n left by the ion pass */
+        if ((flags & kAtoms) && a.pr) {
+            pr0 = a.pr[slot];
+            pr1 = a.pr[ns + slot];
+            pr2 = a.pr[2 * ns + slot];
+        }
+    }
+
     R ea = ex, eb = ey, ec = ez; /* E^n, crystal frame after rotation */
     R da = dx, db = dy, dc = dz;
     rot_fwd<STRICT>(flags, m.cs, m.sn, ea, eb, ec);

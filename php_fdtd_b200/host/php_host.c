@@ -11,6 +11,7 @@
  */
 #define _GNU_SOURCE
 #include "php_host.h"
+#include "php_serve.h"
 
 #include <ctype.h>
 #include <float.h>
@@ -820,5 +821,9 @@ uint64_t php_host_sizeof(const char* n)
     if (!strcmp(n, "php_diag")) return sizeof(php_diag);
     if (!strcmp(n, "php_cfg")) return sizeof(php_cfg);
     if (!strcmp(n, "php_host_material")) return sizeof(php_host_material);
+    if (!strcmp(n, "php_server_desc")) return sizeof(php_server_desc);
+    if (!strcmp(n, "php_dft_request")) return sizeof(php_dft_request);
+    if (!strcmp(n, "php_job_info")) return sizeof(php_job_info);
+    if (!strcmp(n, "php_server_stats")) return sizeof(php_server_stats);
     return 0;
 }

@@ -352,10 +352,10 @@ class Simulation:
         self._ck(self._lib.php_profile_enable(self._ctx, int(bool(enable))))
 
     def profile_read(self) -> dict:
-        ms = np.zeros(4)
-        n = (C.c_int64 * 4)()
+        ms = np.zeros(5)
+        n = (C.c_int64 * 5)()
         self._ck(self._lib.php_profile_read(self._ctx, ms.ctypes.data_as(C.POINTER(C.c_double)), n))
-        names = ("h_sweep", "e_sweep", "probe", "dft")
+        names = ("h_sweep", "e_sweep", "probe", "dft", "ion")
         return {k: {"ms": float(ms[q]), "launches": int(n[q])} for q, k in enumerate(names)}
 
     @property

@@ -424,3 +424,60 @@ def baseline_case(idx: int, tsteps: Optional[int] = None, seed: int = 0, scale: 
                                              np.stack([np.diag([2.7, 2.7, 0.9]), -np.diag([2.7, 2.7, 0.9])]))),
             monitor=f"x={nx // 2},y={nx // 2},z={slab + 1},atom=0,dir=z")
     raise ValueError(f"no single-domain workload {idx}")
+
+
+# ------------------------------------------------------ serving requests
+
+
+def serving_requests(n: int = 256, seed: int = 0, rate_per_s: float = 4.0, edge_range=(64, 192),
+                     steps_range=(3000, 12000), pml: int = 8):
+    """The request stream of the serving configuration: Poisson arrivals at
+    rate_per_s; each grid edge log-uniform in edge_range per axis; 8-cell
+    CPML; steps uniform in steps_range; the 2-atom polar slab of config 0
+    (10 nm cells, slab thickness 40/96 of nz); a sine source at a wavenumber
+    uniform in 700-1600 cm^-1; a Drude-Lorentz tip (config 1 metal at that
+    wavenumber, single-frequency ADE) whose apex sits 5-50 nm above the slab;
+    a running DFT of Ez at the source frequency on the plane two cells above
+    the slab.  Returns dicts with the arrival time and the parameters;
+    ``request_desc`` turns one into a php_desc."""
+    rng = np.random.default_rng(seed + 3000)
+    t = 0.0
+    out = []
+    lo, hi = math.log(edge_range[0]), math.log(edge_range[1])
+    for q in range(n):
+        t += rng.exponential(1.0 / rate_per_s)
+        nx, ny, nz = (int(round(math.exp(rng.uniform(lo, hi)))) for _ in range(3))
+        out.append({"index": q, "arrival": t, "grid": (nx, ny, nz), "pml": pml,
+                    "steps": int(rng.integers(steps_range[0], steps_range[1] + 1)),
+                    "wavenumber": float(rng.uniform(700.0, 1600.0)),
+                    "tip_height_nm": float(rng.uniform(5.0, 50.0))})
+    return out
+
+
+def request_desc(req: dict, precision: str = "fp32", device: int = 0, seed: int = 0):
+    """php_desc (DescHolder) and DFT plane of one serving request."""
+    from .solver import Material, Source, make_desc
+    nx, ny, nz = req["grid"]
+    L = req["pml"]
+    dl = 10e-9
+    dt = dl / (299792458.0 * math.sqrt(3.0)) * 0.99
+    slab = max(1, int(round(40 * nz / 96)))
+    qv, qm, dmm = lattice_2atom(seed)
+    wn = req["wavenumber"]
+    e_tip = drude_lorentz_eps(wn)
+    mats = [Material(),
+            Material(eps_re=(4.9, 0, 0, 0, 4.9, 0, 0, 0, 2.95), natom=2, qezv=qv, qezm=qm, dmm=dmm),
+            Material(eps_re=(e_tip.real, 0, 0, 0, e_tip.real, 0, 0, 0, e_tip.real),
+                     eps_im=(e_tip.imag, 0, 0, 0, e_tip.imag, 0, 0, 0, e_tip.imag), use_ade=1)]
+    med = np.zeros((nx, ny, nz), np.int32)
+    med[:, :, :slab] = 1
+    apex = slab + max(1, int(round(req["tip_height_nm"] * 1e-9 / dl)))
+    top = nz - L - 2
+    if apex < top:
+        med[cone_tip_mask(nx, ny, nz, dl, dl, (nx // 2, ny // 2), apex, 20e-9, 15.0, top_k=top)] = 2
+    f = wn * C_CM
+    zs = min(nz - L - 2, apex + max(2, nz // 4))
+    src = [Source(type=1, x=nx // 2, y=ny // 2, z=max(0, zs), component="z", frequency=f)]
+    holder = make_desc(med, mats, src, dx=dl, dy=dl, dz=dl, dt=dt, pml_thickness=L, precision=precision,
+                       source_frequency=f, device=device)
+    return holder, {"component": "Ez", "z_plane": min(nz - 1, slab + 2), "freqs": [f]}

@@ -23,6 +23,7 @@ def declared_functions(header: Path):
 
 @pytest.mark.parametrize("header,lib", [
     ("include/php_fdtd.h", "php_fdtd_b200/libphpfdtd.so"),
+    ("include/php_serve.h", "php_fdtd_b200/libphpfdtd.so"),
     ("include/php_host.h", "php_fdtd_b200/libphphost.so"),
     ("oracle/php_oracle.h", "oracle/liboracle.so"),
 ])
