@@ -374,14 +374,29 @@ def accuracy_vs_fp64(args, local, steps: int):
 # ------------------------------------------------------ reference / baseline
 
 
-def reference_rate(case_cfg: Path, steps: int, timeout: int = 900):
-    """Runs the reference solver (compiled from its own sources, single
-    rank) on the workload for `steps` time steps; its own loop timer
-    (fdtd.c:3110, 3915) gives the throughput."""
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        return os.cpu_count() or 1
+
+
+def reference_ranks(nz: int) -> int:
+    """MPI ranks for the reference on this host: every core it may use, at
+    most one per two z planes (the reference splits z across ranks)."""
+    return max(1, min(host_cores(), nz // 2))
+
+
+def reference_rate(case_cfg: Path, steps: int, ranks: int = 1, timeout: int = 900):
+    """Runs the reference solver (compiled from its own sources with its
+    release flags) on the workload for `steps` time steps, as `ranks` MPI
+    ranks (forked processes through the shared-memory MPI stand-in); its own
+    loop timer on rank 0 (fdtd.c:3110, 3915) gives the throughput."""
     from oracle import reference_binary
-    exe = reference_binary("fast")
+    exe = reference_binary("mp")
+    env = dict(os.environ, PHP_MPI_NP=str(ranks))
     if not exe.exists():
-        exe = reference_binary("plain")
+        exe, ranks = reference_binary("fast"), 1
     if not exe.exists():
         return None, "reference binary not built (make -C oracle ref)"
     case_dir = case_cfg.parent
@@ -397,12 +412,12 @@ def reference_rate(case_cfg: Path, steps: int, timeout: int = 900):
                 os.symlink(p, dst)
     (run_dir / "case.cfg").write_text(text)
     t0 = time.perf_counter()
-    pr = subprocess.run([str(exe), "case.cfg"], cwd=run_dir, capture_output=True, text=True, timeout=timeout)
+    pr = subprocess.run([str(exe), "case.cfg"], cwd=run_dir, capture_output=True, text=True, timeout=timeout, env=env)
     wall = time.perf_counter() - t0
     m = re.search(r"Simulation completed in ([\d.]+) seconds", pr.stdout)
     if pr.returncode != 0 or not m:
         return None, f"reference run failed rc={pr.returncode}: {pr.stdout[-300:]} {pr.stderr[-300:]}"
-    return {"loop_s": float(m.group(1)), "wall_s": wall, "steps": steps, "exe": exe.name}, None
+    return {"loop_s": float(m.group(1)), "wall_s": wall, "steps": steps, "exe": exe.name, "ranks": ranks}, None
 
 
 def cpu_model():
@@ -415,9 +430,9 @@ def cpu_model():
     return "unknown"
 
 
-def ref_sample_steps(V: int, k: int) -> int:
-    # about 2e8 cell updates (~10-30 s on one core of the reference)
-    return int(max(2, min(k, round(2e8 / V))))
+def ref_sample_steps(V: int, k: int, ranks: int = 1) -> int:
+    # about 2e8 cell updates per rank (~10-30 s of the reference's loop)
+    return int(max(2, min(k, round(2e8 * ranks / V))))
 
 
 def run_reference_arm(args, ws, rank):
@@ -433,11 +448,12 @@ def run_reference_arm(args, ws, rank):
     from php_fdtd_b200.workloads import baseline_case
     spec = baseline_case(WORKLOADS[args.workload], scale=args.scale)
     V = spec.nx * spec.ny * spec.nz
-    steps = ref_sample_steps(V, args.steps)
+    ranks = reference_ranks(spec.nz)
+    steps = ref_sample_steps(V, args.steps, ranks)
     # warm-up sample (page cache, allocator) then the timed sample
     if args.warmup > 0:
-        reference_rate(cfg_path, 1)
-    res, err = reference_rate(cfg_path, steps)
+        reference_rate(cfg_path, 1, ranks)
+    res, err = reference_rate(cfg_path, steps, ranks)
     if res is None:
         print(json.dumps({"impl": "reference", "unavailable": err}))
         return
@@ -448,10 +464,11 @@ def run_reference_arm(args, ws, rank):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "impl": "reference",
         "config": {"workload": workload_name(args), "grid": [spec.nx, spec.ny, spec.nz], "cells": V},
-        "cpu_baseline": {"value": round(rate, 6), "unit": "Gcell-updates/s", "cores": 1, "kind": "reference",
+        "cpu_baseline": {"value": round(rate, 6), "unit": "Gcell-updates/s", "cores": res["ranks"], "kind": "reference",
                          "sample": f"{steps} time steps of the full {spec.nx}x{spec.ny}x{spec.nz} domain, reference "
-                                   f"solver ({res['exe']}, -Ofast, one MPI rank through the single-rank MPI stub), "
-                                   f"timed by its own loop timer; CPU {cpu_model()}"},
+                                   f"solver ({res['exe']}, -Ofast -funroll-loops, {res['ranks']} MPI ranks as processes "
+                                   f"through the shared-memory MPI stand-in, {host_cores()} host cores usable), timed "
+                                   f"by its own loop timer; CPU {cpu_model()}"},
         "e2e": {"value": round(rate, 6), "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -596,13 +613,15 @@ def main():
         cpu = None
         if not args.no_cpu_baseline and ws == 1:
             case_dir = Path(args.case_dir or tempfile.gettempdir()) / f"php_bench_{args.workload}_{args.scale}_r{rank}"
-            steps = ref_sample_steps(r["V"], args.steps)
-            res, err = reference_rate(case_dir / "case.cfg", steps)
+            ranks = reference_ranks(cfg.nz)
+            steps = ref_sample_steps(r["V"], args.steps, ranks)
+            res, err = reference_rate(case_dir / "case.cfg", steps, ranks)
             if res:
-                cpu = {"value": round(r["V"] * steps / res["loop_s"] / 1e9, 6), "unit": "Gcell-updates/s", "cores": 1,
-                       "kind": "reference",
-                       "sample": f"{steps} time steps of the full domain, reference solver {res['exe']} (one MPI rank "
-                                 f"through the single-rank stub, its own loop timer); CPU {cpu_model()}"}
+                cpu = {"value": round(r["V"] * steps / res["loop_s"] / 1e9, 6), "unit": "Gcell-updates/s",
+                       "cores": res["ranks"], "kind": "reference",
+                       "sample": f"{steps} time steps of the full domain, reference solver {res['exe']} "
+                                 f"({res['ranks']} MPI ranks as processes through the shared-memory MPI stand-in, its "
+                                 f"own loop timer); CPU {cpu_model()}"}
             else:
                 cpu = {"value": None, "unit": "Gcell-updates/s", "cores": 1, "kind": "reference", "sample": err}
         line = {

@@ -50,8 +50,10 @@ def lib():
 
 
 def reference_binary(kind: str = "wide") -> Path:
-    """oracle/_ref/fdtd_ref{,_wide,_fast}: the reference solver itself."""
-    name = {"plain": "fdtd_ref", "wide": "fdtd_ref_wide", "fast": "fdtd_ref_fast"}[kind]
+    """oracle/_ref/fdtd_ref{,_wide,_fast,_mp}: the reference solver itself
+    (_mp: release flags, PHP_MPI_NP ranks through the shared-memory MPI
+    stand-in of mpi_shm/mpi.h)."""
+    name = {"plain": "fdtd_ref", "wide": "fdtd_ref_wide", "fast": "fdtd_ref_fast", "mp": "fdtd_ref_mp"}[kind]
     return HERE / "_ref" / name
 
 

@@ -55,7 +55,8 @@ struct php_ctx {
     int64_t plane = 0, ncell_dev = 0;
     int zchunk = 1;
     int n3max = 0, namax_tpl = 0;
-    int64_t nslot = 0;
+    int64_t nslot = 0;           /* pool slots, padded to a multiple of 32 */
+    int num_sms = 148;
     bool any_ade = false, any_atoms = false;
     cudaStream_t stream = nullptr;
     std::string err;
@@ -68,6 +69,7 @@ struct php_ctx {
     uint8_t* mat = nullptr;
     int32_t* slot = nullptr;
     int64_t* slot_cell = nullptr;
+    uint8_t* slot_mat = nullptr;
     int32_t* slot_n3 = nullptr;
     void *P = nullptr, *Po = nullptr, *r = nullptr, *v = nullptr;
     void* mc = nullptr;          /* MatCoef<R>[nmat] */
@@ -130,6 +132,10 @@ struct php_ctx {
     void* Pr = nullptr;          /* [3][nslot] */
     void* ion_dmm = nullptr;     /* CUDA-core kernel: [np][np] R */
     void* ion_bsplit = nullptr;  /* tensor kernel: DMM hi, lo bf16 images */
+    bool ion_pipe = false;       /* TMA-fed pass (ion_pipe) */
+    IonMaps ion_maps;
+    int n3_ion = 0;
+    int ion_off_ref = 0;
 };
 
 /* ------------------------------------------------------------------ utils */
@@ -527,6 +533,8 @@ static void launch_ions(php_ctx* ctx)
     a.pr = (R*)ctx->Pr;
     a.slot_cell = ctx->slot_cell;
     a.slot_n3 = ctx->slot_n3;
+    a.slot_mat = ctx->slot_mat;
+    a.ion_off_ref = ctx->ion_off_ref;
     a.mat = ctx->mat;
     a.mc = (const MatCoef<R>*)ctx->mc;
     a.ion_coef = (const R*)ctx->ion_coef;
@@ -536,23 +544,32 @@ static void launch_ions(php_ctx* ctx)
     a.ntiles = (int32_t)((ctx->nslot + kIonTile - 1) / kIonTile);
     a.dt = ctx->d.dt;
     a.err = ctx->err_flag;
-    const int grid = (int)std::min<int64_t>(a.ntiles, 148 * 4);
     cudaStream_t st = ctx->stream;
-    if constexpr (sizeof(R) == 4) {
-        switch (ctx->ion_np) {
-        case 16: ion_update_tc<16><<<grid, kIonTile, IonTc<16>::SMEM, st>>>(a); break;
-        case 32: ion_update_tc<32><<<grid, kIonTile, IonTc<32>::SMEM, st>>>(a); break;
-        case 48: ion_update_tc<48><<<grid, kIonTile, IonTc<48>::SMEM, st>>>(a); break;
-        default: ion_update_tc<64><<<grid, kIonTile, IonTc<64>::SMEM, st>>>(a); break;
+    if (ctx->ion_pipe) {
+        /* one persistent CTA per SM */
+        const int grid = (int)std::min<int64_t>(a.ntiles, ctx->num_sms);
+        const int n3 = ctx->n3_ion;
+#define PHP_ION_PIPE(NP, S) \
+    ion_pipe<R, NP, S><<<grid, IonPipe<R, NP, S>::THREADS, IonPipe<R, NP, S>::SMEM, st>>>(a, ctx->ion_maps, n3)
+        if constexpr (sizeof(R) == 4) {
+            switch (ctx->ion_np) {
+            case 16: PHP_ION_PIPE(16, 3); break;
+            case 32: PHP_ION_PIPE(32, 3); break;
+            case 48: PHP_ION_PIPE(48, 3); break;
+            default: PHP_ION_PIPE(64, 2); break;
+            }
+        } else {
+            switch (ctx->ion_np) {
+            case 16: PHP_ION_PIPE(16, 2); break;
+            case 32: PHP_ION_PIPE(32, 2); break;
+            default: PHP_ION_PIPE(48, 2); break;
+            }
         }
-    } else {
-        switch (ctx->ion_np) {
-        case 16: ion_update_cc<R, 16><<<grid, kIonTile, 0, st>>>(a); break;
-        case 32: ion_update_cc<R, 32><<<grid, kIonTile, 0, st>>>(a); break;
-        case 48: ion_update_cc<R, 48><<<grid, kIonTile, 0, st>>>(a); break;
-        default: ion_update_cc<R, 64><<<grid, kIonTile, 0, st>>>(a); break;
-        }
+#undef PHP_ION_PIPE
+        return;
     }
+    const int grid = (int)std::min<int64_t>(a.ntiles, 148 * 4);
+    ion_update_cc<R, 64><<<grid, kIonTile, 0, st>>>(a);
 }
 
 template <typename R, bool STRICT, int NA>
@@ -798,6 +815,13 @@ static int alloc_step_inputs(php_ctx* ctx, int row)
     return PHP_OK;
 }
 
+template <typename R, int NP, int S>
+static cudaError_t ion_pipe_attr()
+{
+    return cudaFuncSetAttribute(ion_pipe<R, NP, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)IonPipe<R, NP, S>::SMEM);
+}
+
 /* bf16 bits of x, rounded to nearest even (finite inputs) */
 static uint16_t bf16_bits(float x)
 {
@@ -818,7 +842,7 @@ static double bf16_value(uint16_t b)
 /* Many-atom cells (3N >= 24, one DMM shared by every atom material) get the
  * ion pass of php_ions.cuh in the fast FP64 and FP32 paths; PHP_IONS=fused
  * keeps the update inside the E sweep (for A/B timing). */
-static int setup_ion_pass(php_ctx* ctx, const std::vector<MatD>& mats, const php_desc& d)
+static int setup_ion_pass(php_ctx* ctx, const std::vector<MatD>& mats, const std::vector<int>& ion_off, const php_desc& d)
 {
     const char* iv = getenv("PHP_IONS");
     if ((iv && !strcmp(iv, "fused")) || ctx->prec == PHP_PREC_FP64_STRICT || ctx->n3max < 24 || ctx->n3max > 64)
@@ -855,10 +879,6 @@ static int setup_ion_pass(php_ctx* ctx, const std::vector<MatD>& mats, const php
         if ((rc = dalloc(ctx, &ctx->ion_bsplit, img.size() * 2))) return rc;
         CK(cudaMemcpyAsync(ctx->ion_bsplit, img.data(), img.size() * 2, cudaMemcpyHostToDevice, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
-        cudaError_t e = cudaSuccess;
-        if (np == 64)
-            e = cudaFuncSetAttribute(ion_update_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)IonTc<64>::SMEM);
-        if (e != cudaSuccess) return fail(ctx, PHP_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
         ctx->ion_tc = true;
     } else {
         std::vector<double> pad((size_t)np * np, 0.0);
@@ -870,6 +890,23 @@ static int setup_ion_pass(php_ctx* ctx, const std::vector<MatD>& mats, const php
     }
     ctx->ion_np = np;
     ctx->ion_split = true;
+    ctx->n3_ion = n3;
+    ctx->ion_off_ref = ion_off[ref];
+    ctx->ion_pipe = ctx->prec == PHP_PREC_FP32 ? np <= 64 : np <= 48;
+    if (ctx->ion_pipe) {
+        const CUtensorMapDataType dt = ctx->prec == PHP_PREC_FP32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+        rc = encode_map(ctx, &ctx->ion_maps.r, ctx->r, dt, rs, (uint64_t)ctx->nslot, (uint64_t)n3, 1, kIonTile, (uint32_t)n3);
+        if (!rc) rc = encode_map(ctx, &ctx->ion_maps.v, ctx->v, dt, rs, (uint64_t)ctx->nslot, (uint64_t)n3, 1, kIonTile, (uint32_t)n3);
+        if (rc) return rc;
+        cudaError_t e;
+        if (ctx->prec == PHP_PREC_FP32)
+            e = np == 16 ? ion_pipe_attr<float, 16, 3>() : np == 32 ? ion_pipe_attr<float, 32, 3>()
+              : np == 48 ? ion_pipe_attr<float, 48, 3>() : ion_pipe_attr<float, 64, 2>();
+        else
+            e = np == 16 ? ion_pipe_attr<double, 16, 2>() : np == 32 ? ion_pipe_attr<double, 32, 2>()
+                         : ion_pipe_attr<double, 48, 2>();
+        if (e != cudaSuccess) return fail(ctx, PHP_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+    }
     return PHP_OK;
 }
 
@@ -900,6 +937,7 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(ctx, PHP_ERR_NODEVICE, "no CUDA device visible");
     if (d.device < 0 || d.device >= ndev) return fail(ctx, PHP_ERR_INPUT, "device %d not present", d.device);
     CK(cudaSetDevice(d.device));
+    CK(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, d.device));
     CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
 
     /* materials */
@@ -947,6 +985,13 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
                     if (mats[id].flags & kAtoms) ctx->any_atoms = true;
                 }
             }
+    /* pad the pool to a multiple of 32 slots (16-byte rows for the tensor
+     * maps of the ion pass); padding slots have no atoms */
+    const int64_t nreal = (int64_t)slot_cell.size();
+    while (nreal > 0 && slot_cell.size() % 32) {
+        slot_cell.push_back(slot_cell.back());
+        slot_n3.push_back(0);
+    }
     ctx->nslot = (int64_t)slot_cell.size();
     ctx->n3max = n3max;
     const int namax = n3max / 3;
@@ -1003,7 +1048,7 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
     CK(cudaMemcpyAsync(ctx->mat, mat_dev.data(), mat_dev.size(), cudaMemcpyHostToDevice, ctx->stream));
     if (ctx->nslot > 0) {
         slot_dev.assign((size_t)ctx->ncell_dev, -1);
-        for (int64_t s = 0; s < ctx->nslot; s++) slot_dev[slot_cell[s]] = (int32_t)s;
+        for (int64_t s = 0; s < nreal; s++) slot_dev[slot_cell[s]] = (int32_t)s;
         rc = dalloc(ctx, (void**)&ctx->slot, slot_dev.size() * sizeof(int32_t));
         if (rc) return rc;
         CK(cudaMemcpyAsync(ctx->slot, slot_dev.data(), slot_dev.size() * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
@@ -1014,6 +1059,12 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
         rc = dalloc(ctx, (void**)&ctx->slot_n3, slot_n3.size() * sizeof(int32_t));
         if (rc) return rc;
         CK(cudaMemcpyAsync(ctx->slot_n3, slot_n3.data(), slot_n3.size() * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
+        std::vector<uint8_t> slot_mat(slot_cell.size(), 0);
+        for (int64_t s = 0; s < nreal; s++) slot_mat[s] = mat_dev[slot_cell[s]];
+        rc = dalloc(ctx, (void**)&ctx->slot_mat, slot_mat.size());
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(ctx->slot_mat, slot_mat.data(), slot_mat.size(), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream)); /* the host vectors go out of scope */
     }
     if (ctx->any_ade) {
         if ((rc = dalloc(ctx, &ctx->P, 3 * (size_t)ctx->nslot * rs))) return rc;
@@ -1023,7 +1074,7 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
         if ((rc = dalloc(ctx, &ctx->r, (size_t)n3max * ctx->nslot * rs))) return rc;
         if ((rc = dalloc(ctx, &ctx->v, (size_t)n3max * ctx->nslot * rs))) return rc;
     }
-    if ((rc = setup_ion_pass(ctx, mats, d))) return rc;
+    if ((rc = setup_ion_pass(ctx, mats, ion_off, d))) return rc;
 
     AxisD axes[3];
     derive_axis(d, nx, d.dx, false, axes[0]);

@@ -17,16 +17,18 @@
  * step.  The arithmetic is the reference's; only its rounding order differs
  * from the fused form (FP64: within 1e-10 of the reference).
  *
- *  ion_update_cc  CUDA cores, FP64 (the fast plain path): DMM in shared
- *                 memory, one cell per thread.
- *  ion_update_tc  FP32 mixed path on the 5th-generation tensor cores: per
- *                 128-cell tile, r is split into bf16 hi + lo, DMM likewise
- *                 (host), and D = r_hi DMM_hi^T + r_hi DMM_lo^T + r_lo DMM_hi^T
- *                 accumulates in FP32 in tensor memory (tcgen05.mma
- *                 kind::f16, M = 128, N = K = 3N padded to 16); the
- *                 epilogue reads D with tcgen05.ld and does the update.  The
- *                 dropped r_lo DMM_lo term and the bf16 representation leave
- *                 about 2^-17 relative error in DMM . r.
+ *  ion_pipe       the pass proper: a TMA-fed ring of pool tiles, two
+ *                 consumer warpgroups.  FP32 (mixed path) on the 5th-generation
+ *                 tensor cores: per 128-cell tile, r is split into bf16 hi + lo,
+ *                 DMM likewise (host), and D = r_hi DMM_hi^T + r_hi DMM_lo^T +
+ *                 r_lo DMM_hi^T accumulates in FP32 in tensor memory
+ *                 (tcgen05.mma kind::f16, M = 128, N = K = 3N padded to 16);
+ *                 the epilogue reads D with tcgen05.ld and does the update.
+ *                 The dropped r_lo DMM_lo term and the bf16 representation
+ *                 leave about 2^-17 relative error in DMM . r.  FP64 (fast
+ *                 plain path): FMA chains against DMM in shared memory.
+ *  ion_update_cc  plain loads, FP64, one cell per thread: used where the
+ *                 FP64 ring does not fit in shared memory (3N > 48).
  */
 #pragma once
 
@@ -40,6 +42,7 @@ struct IonArgs {
     R *r, *v, *pr;               /* pools [3N][nslot], Pr [3][nslot] */
     const int64_t* slot_cell;
     const int32_t* slot_n3;
+    const uint8_t* slot_mat;     /* material id per slot */
     const uint8_t* mat;
     const MatCoef<R>* mc;
     const R* ion_coef;
@@ -47,6 +50,7 @@ struct IonArgs {
     const uint32_t* bsplit;      /* DMM hi, lo as bf16 in the UMMA K-major layout (tensor kernel) */
     int64_t nslot;
     int32_t ntiles;
+    int32_t ion_off_ref;         /* the lattice's QeZV/QeZM block, staged in shared memory */
     double dt;
     int32_t* err;
 };
@@ -160,173 +164,363 @@ __device__ __forceinline__ uint32_t bf16x2_bits(__nv_bfloat16 lo_half, __nv_bflo
     return (uint32_t)__bfloat16_as_ushort(lo_half) | ((uint32_t)__bfloat16_as_ushort(hi_half) << 16);
 }
 
-template <int NP>
-struct IonTc {
-    static constexpr int COLS = NP <= 32 ? 32 : NP <= 64 ? 64 : 128;   /* TMEM columns */
-    static constexpr uint32_t A_BYTES = kIonTile * NP * 2;
-    static constexpr uint32_t B_BYTES = NP * NP * 2;
-    /* A_hi, A_lo, B_hi, B_lo, then the barrier and the TMEM address */
-    static constexpr uint32_t SMEM = 1024 + 2 * A_BYTES + 2 * B_BYTES + 64;
+/* ------------------------------------------------- pipelined ion pass
+ *
+ * One CTA per SM, persistent over 128-cell tiles.  Warp 8 streams the r
+ * and v tiles of the pool (box 128 cells x 3N, cp.async.bulk.tensor, no
+ * multicast) and the tiles' slot indices (cp.async.bulk) into a ring of S
+ * stages; two consumer warpgroups take alternate tiles, so that one group's
+ * tensor-core round trip or E gather overlaps the other's epilogue.  The
+ * updated r, v go back from the stage with a tensor store.  FP32: DMM . r as
+ * BF16 x 3 on tcgen05 (each group its own A buffers and TMEM columns); FP64:
+ * CUDA-core FMA chains against DMM in shared memory.
+ */
+struct IonMaps {
+    CUtensorMap r, v; /* pool [3N][ns] as (x = slot, y = coordinate), box 128 x 3N */
 };
 
 template <int NP>
-__global__ void __launch_bounds__(kIonTile, 4) ion_update_tc(const IonArgs<float> a)
+__host__ __device__ constexpr int ion_cols() { return NP <= 32 ? 32 : 64; }
+
+template <typename R, int NP, int S>
+struct IonPipe {
+    static constexpr bool TC = sizeof(R) == 4;
+    static constexpr int GROUPS = 2, CONSUMERS = GROUPS * kIonTile, THREADS = CONSUMERS + 32;
+    static constexpr uint32_t BOX = kIonTile * NP * sizeof(R);      /* one array's tile, NP rows */
+    /* per stage: r, v, then the slots' cell offsets (int64, 1024 B), atom
+     * coordinate counts (int32, 512 B) and material ids (uint8, 128 B) */
+    static constexpr uint32_t IDX = 2048;
+    static constexpr uint32_t STAGE = 2 * BOX + IDX;
+    static constexpr uint32_t A_BYTES = kIonTile * NP * 2;           /* bf16 rows of one group */
+    static constexpr uint32_t B_BYTES = NP * NP * 2;
+    static constexpr uint32_t OPS = TC ? GROUPS * 2 * A_BYTES + 2 * B_BYTES : NP * NP * sizeof(R);
+    static constexpr uint32_t COEF = 2 * 3 * NP * sizeof(R);         /* QeZV, QeZM: 9N each, 9N <= 3 NP */
+    static constexpr uint32_t SMEM = 1024 + S * STAGE + OPS + COEF + 256;
+};
+
+__device__ __forceinline__ void named_sync(int id, int n)
 {
-    using T = IonTc<NP>;
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+
+/* barrier `id` over n threads that also ORs a predicate across them */
+__device__ __forceinline__ bool named_sync_or(int id, int n, bool v)
+{
+    uint32_t r;
+    asm volatile("{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, %2, %3, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+                 : "=r"(r)
+                 : "r"((uint32_t)v), "r"(id), "r"(n)
+                 : "memory");
+    return r != 0;
+}
+
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, const void* src, int x, int y, int z)
+{
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];"
+                 ::"l"(map), "r"(smem_addr(src)), "r"(x), "r"(y), "r"(z)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+/* untiled bulk copy global -> shared, completing on an mbarrier (both
+ * addresses 16-byte aligned, size a multiple of 16) */
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+template <typename R, int NP, int S>
+__global__ void __launch_bounds__(IonPipe<R, NP, S>::THREADS, 1)
+    ion_pipe(const __grid_constant__ IonArgs<R> a, const __grid_constant__ IonMaps maps, int32_t n3)
+{
+    using P = IonPipe<R, NP, S>;
     static_assert(NP % 16 == 0 && NP >= 16 && NP <= 64, "3N padded to 16..64");
     extern __shared__ __align__(128) unsigned char dyn_smem[];
     unsigned char* base = dyn_smem + ((1024u - (smem_addr(dyn_smem) & 1023u)) & 1023u);
-    unsigned char* Ahi = base;
-    unsigned char* Alo = base + T::A_BYTES;
-    unsigned char* Bhi = base + 2 * T::A_BYTES;
-    unsigned char* Blo = Bhi + T::B_BYTES;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(Blo + T::B_BYTES);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
+    unsigned char* stages = base;
+    unsigned char* ops = base + S * P::STAGE;
+    R* coef = reinterpret_cast<R*>(ops + P::OPS);
+    uint64_t* full = reinterpret_cast<uint64_t*>(ops + P::OPS + P::COEF);
+    uint64_t* empty = full + S;
+    uint64_t* mma_bar = empty + S;                                 /* one per group */
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_bar + P::GROUPS);
+    volatile int32_t* consumed = reinterpret_cast<volatile int32_t*>(tmem_slot + 1);
 
     const int tid = threadIdx.x, warp = tid >> 5;
-    /* B operands: host-prepared bf16 images, copied once */
+    const int mine = a.ntiles > (int)blockIdx.x ? (a.ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+
+    /* DMM (bf16 images for the tensor cores, or the padded FP64 matrix) and
+     * the lattice's QeZV, QeZM (cells of other materials read global) */
     {
-        const uint4* src = reinterpret_cast<const uint4*>(a.bsplit);
-        uint4* dst = reinterpret_cast<uint4*>(Bhi);
-        for (int t = tid; t < (int)(2 * T::B_BYTES / 16); t += kIonTile) dst[t] = src[t];
+        const uint4* src = P::TC ? reinterpret_cast<const uint4*>(a.bsplit) : reinterpret_cast<const uint4*>(a.dmm);
+        unsigned char* dst0 = P::TC ? ops + P::GROUPS * 2 * P::A_BYTES : ops;
+        const int n16 = (int)((P::TC ? 2 * P::B_BYTES : NP * NP * sizeof(R)) / 16);
+        uint4* dst = reinterpret_cast<uint4*>(dst0);
+        for (int t = tid; t < n16; t += P::THREADS) dst[t] = src[t];
+        for (int t = tid; t < 6 * n3; t += P::THREADS) coef[t] = a.ion_coef[a.ion_off_ref + t];
     }
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
-                     "r"(T::COLS));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    if constexpr (P::TC) {
+        if (warp == 0) {
+            asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
+                         "r"(P::GROUPS * ion_cols<NP>()));
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+        }
     }
     if (tid == 0) {
-        mbar_init(bar, 1);
+        for (int q = 0; q < S; ++q) {
+            mbar_init(&full[q], 1);
+            mbar_init(&empty[q], 1);
+        }
+        for (int g = 0; g < P::GROUPS; ++g) mbar_init(&mma_bar[g], 1);
+        *consumed = 0;
         fence_barrier_init();
     }
-    fence_proxy_async_smem(); /* B images written with generic stores */
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    fence_proxy_async_smem();
+    if constexpr (P::TC) asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const uint32_t tmem = *tmem_slot;
-    const uint32_t idesc = umma_idesc_bf16(kIonTile, NP);
-    const uint32_t sa_hi = smem_addr(Ahi), sa_lo = smem_addr(Alo), sb_hi = smem_addr(Bhi), sb_lo = smem_addr(Blo);
-    const float dt = (float)a.dt;
-    const int64_t ns = a.nslot;
-    bool ok = true;
-    uint32_t phase = 0;
+    if constexpr (P::TC) asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem0 = P::TC ? *tmem_slot : 0u;
+    const uint32_t tx_bytes = 2u * kIonTile * (uint32_t)n3 * (uint32_t)sizeof(R);
+    bool failed = false;
 
-    for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
-        const int64_t s = (int64_t)tile * kIonTile + tid;
-        const bool valid = s < ns;
-        const int n3 = valid ? a.slot_n3[s] : 0;
-        /* the dependent gather slot -> cell -> material -> E goes first */
-        float e0 = 0.f, e1 = 0.f, e2 = 0.f;
-        const MatCoef<float>* mp = nullptr;
-        if (n3) mp = &ion_cell_e(a, s, e0, e1, e2);
-        /* r of this cell: registers (FP32) and bf16 hi/lo rows of A */
-        float rold[NP];
-#pragma unroll
-        for (int q = 0; q < NP; ++q) rold[q] = q < n3 ? a.r[(int64_t)q * ns + s] : 0.f;
-#pragma unroll
-        for (int kc = 0; kc < NP / 8; ++kc) {
-            uint32_t h[4], l[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const float x0 = rold[kc * 8 + 2 * u], x1 = rold[kc * 8 + 2 * u + 1];
-                const __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
-                const __nv_bfloat16 l0 = __float2bfloat16_rn(x0 - __bfloat162float(h0));
-                const __nv_bfloat16 l1 = __float2bfloat16_rn(x1 - __bfloat162float(h1));
-                h[u] = bf16x2_bits(h0, h1);
-                l[u] = bf16x2_bits(l0, l1);
+    if (warp == P::GROUPS * 4) {
+        /* ------------------------------------------------------ producer */
+        if ((tid & 31) == 0) {
+            int issued = 0;
+            for (int k = 0; k < mine; ++k) {
+                const int st = k % S;
+                if (k >= S && !mbar_wait(&empty[st], ((k / S) - 1) & 1)) {
+                    failed = true;
+                    break;
+                }
+                const int x = ((int)blockIdx.x + k * (int)gridDim.x) * kIonTile;
+                unsigned char* b = stages + st * P::STAGE;
+                /* slots left in this tile: a multiple of 32 (the pool is padded) */
+                const uint32_t nrem = (uint32_t)min((int64_t)kIonTile, a.nslot - x);
+                mbar_arrive_expect_tx(&full[st], tx_bytes + nrem * 13u);
+                tma_load_3d(b, &maps.r, &full[st], x, 0, 0);
+                tma_load_3d(b + P::BOX, &maps.v, &full[st], x, 0, 0);
+                bulk_load(b + 2 * P::BOX, a.slot_cell + x, nrem * 8u, &full[st]);
+                bulk_load(b + 2 * P::BOX + 1024, a.slot_n3 + x, nrem * 4u, &full[st]);
+                bulk_load(b + 2 * P::BOX + 1536, a.slot_mat + x, nrem, &full[st]);
+                issued = k + 1;
             }
-            const uint32_t off = umma_kmajor_off(tid, kc * 8, kIonTile);
-            *reinterpret_cast<uint4*>(Ahi + off) = make_uint4(h[0], h[1], h[2], h[3]);
-            *reinterpret_cast<uint4*>(Alo + off) = make_uint4(l[0], l[1], l[2], l[3]);
-        }
-        fence_proxy_async_smem();
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll
-            for (int ks = 0; ks < NP / 16; ++ks) {
-                const uint32_t ao = umma_kmajor_off(0, ks * 16, kIonTile), bo = umma_kmajor_off(0, ks * 16, NP);
-                const uint64_t dah = umma_smem_desc(sa_hi + ao, kIonTile * 16, 128);
-                const uint64_t dal = umma_smem_desc(sa_lo + ao, kIonTile * 16, 128);
-                const uint64_t dbh = umma_smem_desc(sb_hi + bo, NP * 16, 128);
-                const uint64_t dbl = umma_smem_desc(sb_lo + bo, NP * 16, 128);
-                const uint32_t acc0 = ks > 0 ? 1u : 0u;
-                asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-                             " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
-                             ::"r"(tmem), "l"(dah), "l"(dbh), "r"(idesc), "r"(acc0));
-                asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-                             " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
-                             ::"r"(tmem), "l"(dah), "l"(dbl), "r"(idesc), "r"(1u));
-                asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-                             " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
-                             ::"r"(tmem), "l"(dal), "l"(dbh), "r"(idesc), "r"(1u));
+            if (failed) {
+                atomicExch(a.err, 1);
+                /* loads issued and not consumed land before the CTA leaves */
+                for (int k = *consumed; k < issued; ++k) mbar_wait(&full[k % S], (k / S) & 1);
             }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             smem_addr(bar))
-                         : "memory");
         }
-        const bool got = mbar_wait(bar, phase);
-        phase ^= 1u;
-        if (__syncthreads_or(!got)) {
-            ok = false;
-            break;
-        }
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-
-        /* epilogue: this thread's row of D, 16 columns at a time */
-        float p0 = 0.f, p1 = 0.f, p2 = 0.f;
-        const float* qv = n3 ? a.ion_coef + mp->ion_off : nullptr;
-        const float* qm = n3 ? qv + 3 * n3 : nullptr;
+    } else {
+        /* ------------------------------------------------------ consumers */
+        const int g = warp >> 2, gt = tid & (kIonTile - 1), bar_id = 1 + g;
+        const int64_t ns = a.nslot;
+        const R dt = R(a.dt);
+        unsigned char* Ahi = ops + g * 2 * P::A_BYTES;
+        unsigned char* Alo = Ahi + P::A_BYTES;
+        const unsigned char* Bhi = ops + P::GROUPS * 2 * P::A_BYTES;
+        const unsigned char* Blo = Bhi + P::B_BYTES;
+        const R* Dsm = reinterpret_cast<const R*>(ops);
+        const uint32_t tmem = tmem0 + (uint32_t)(g * ion_cols<NP>());
+        uint32_t mphase = 0;
+        for (int k = g; k < mine; k += P::GROUPS) {
+            const int st = k % S;
+            const int64_t s = (int64_t)((int)blockIdx.x + k * (int)gridDim.x) * kIonTile + gt;
+            const bool got = mbar_wait(&full[st], (k / S) & 1);
+            if (named_sync_or(bar_id, kIonTile, !got)) {
+                failed = true;
+                break;
+            }
+            unsigned char* sb = stages + st * P::STAGE;
+            R* rs = reinterpret_cast<R*>(sb);
+            R* vs = reinterpret_cast<R*>(sb + P::BOX);
+            const int n3c = s < ns ? reinterpret_cast<const int32_t*>(sb + 2 * P::BOX + 1024)[gt] : 0;
+            R e0 = R(0), e1 = R(0), e2 = R(0);
+            const MatCoef<R>* mp = nullptr;
+            if (n3c) {
+                const int64_t c = reinterpret_cast<const int64_t*>(sb + 2 * P::BOX)[gt];
+                mp = &a.mc[(sb + 2 * P::BOX + 1536)[gt]];
+                e0 = a.ex[c];
+                e1 = a.ey[c];
+                e2 = a.ez[c];
+                rot_fwd<false>(mp->flags, mp->cs, mp->sn, e0, e1, e2);
+            }
+            R p0 = R(0), p1 = R(0), p2 = R(0);
+            const R* qv = n3c ? (mp->ion_off == a.ion_off_ref ? coef : a.ion_coef + mp->ion_off) : nullptr;
+            const R* qm = n3c ? qv + 3 * n3c : nullptr;
+            if constexpr (P::TC) {
+                /* A rows (this cell) as bf16 hi + lo */
 #pragma unroll
-        for (int cb = 0; cb < NP; cb += 16) {
-            uint32_t d[16];
-            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb;
-            asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-                         : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]),
-                           "=r"(d[7]), "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]),
-                           "=r"(d[14]), "=r"(d[15])
-                         : "r"(taddr));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                for (int kc = 0; kc < NP / 8; ++kc) {
+                    uint32_t h[4], l[4];
 #pragma unroll
-            for (int u = 0; u < 16; ++u) {
-                const int q = cb + u;
-                if (q < n3) {
-                    const int at = q / 3, dd = q - 3 * at;
-                    const float acc = ldg(qm + at * 9 + dd) * e0 + ldg(qm + at * 9 + 3 + dd) * e1 +
-                                      ldg(qm + at * 9 + 6 + dd) * e2 - __uint_as_float(d[u]);
-                    const int64_t o = (int64_t)q * ns + s;
-                    const float vq = a.v[o];
-                    const float rn = rold[q] + (vq * dt + 0.5f * acc * dt * dt);
-                    a.r[o] = rn;
-                    a.v[o] = vq + acc * dt;
-                    p0 += ldg(qv + at * 9 + dd) * rn;
-                    p1 += ldg(qv + at * 9 + 3 + dd) * rn;
-                    p2 += ldg(qv + at * 9 + 6 + dd) * rn;
+                    for (int u = 0; u < 4; ++u) {
+                        const int q = kc * 8 + 2 * u;
+                        const float x0 = q < n3 ? (float)rs[q * kIonTile + gt] : 0.f;
+                        const float x1 = q + 1 < n3 ? (float)rs[(q + 1) * kIonTile + gt] : 0.f;
+                        const __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
+                        const __nv_bfloat16 l0 = __float2bfloat16_rn(x0 - __bfloat162float(h0));
+                        const __nv_bfloat16 l1 = __float2bfloat16_rn(x1 - __bfloat162float(h1));
+                        h[u] = bf16x2_bits(h0, h1);
+                        l[u] = bf16x2_bits(l0, l1);
+                    }
+                    const uint32_t off = umma_kmajor_off(gt, kc * 8, kIonTile);
+                    *reinterpret_cast<uint4*>(Ahi + off) = make_uint4(h[0], h[1], h[2], h[3]);
+                    *reinterpret_cast<uint4*>(Alo + off) = make_uint4(l[0], l[1], l[2], l[3]);
+                }
+                fence_proxy_async_smem();
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                named_sync(bar_id, kIonTile);
+                if (gt == 0) {
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t idesc = umma_idesc_bf16(kIonTile, NP);
+                    const uint32_t sa_hi = smem_addr(Ahi), sa_lo = smem_addr(Alo);
+                    const uint32_t sb_hi = smem_addr(Bhi), sb_lo = smem_addr(Blo);
+#pragma unroll
+                    for (int ks = 0; ks < NP / 16; ++ks) {
+                        const uint32_t ao = umma_kmajor_off(0, ks * 16, kIonTile), bo = umma_kmajor_off(0, ks * 16, NP);
+                        const uint64_t dah = umma_smem_desc(sa_hi + ao, kIonTile * 16, 128);
+                        const uint64_t dal = umma_smem_desc(sa_lo + ao, kIonTile * 16, 128);
+                        const uint64_t dbh = umma_smem_desc(sb_hi + bo, NP * 16, 128);
+                        const uint64_t dbl = umma_smem_desc(sb_lo + bo, NP * 16, 128);
+                        const uint32_t acc0 = ks > 0 ? 1u : 0u;
+                        asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                                     " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+                                     ::"r"(tmem), "l"(dah), "l"(dbh), "r"(idesc), "r"(acc0));
+                        asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                                     " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+                                     ::"r"(tmem), "l"(dah), "l"(dbl), "r"(idesc), "r"(1u));
+                        asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                                     " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+                                     ::"r"(tmem), "l"(dal), "l"(dbh), "r"(idesc), "r"(1u));
+                    }
+                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                     smem_addr(&mma_bar[g]))
+                                 : "memory");
+                }
+                const bool done = mbar_wait(&mma_bar[g], mphase);
+                mphase ^= 1u;
+                if (named_sync_or(bar_id, kIonTile, !done)) {
+                    failed = true;
+                    if (gt == 0) mbar_wait(&mma_bar[g], mphase ^ 1u); /* the MMAs in flight finish first */
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+                for (int cb = 0; cb < NP; cb += 16) {
+                    uint32_t d[16];
+                    const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)cb;
+                    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                                 : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]),
+                                   "=r"(d[7]), "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]),
+                                   "=r"(d[14]), "=r"(d[15])
+                                 : "r"(taddr));
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                    for (int u = 0; u < 16; ++u) {
+                        const int q = cb + u;
+                        if (q < n3c) {
+                            const int at = q / 3, dd = q - 3 * at;
+                            const R acc = qm[at * 9 + dd] * e0 + qm[at * 9 + 3 + dd] * e1 + qm[at * 9 + 6 + dd] * e2 -
+                                          __uint_as_float(d[u]);
+                            const int o = q * kIonTile + gt;
+                            const R vq = vs[o];
+                            const R rn = rs[o] + (vq * dt + R(0.5) * acc * dt * dt);
+                            rs[o] = rn;
+                            vs[o] = vq + acc * dt;
+                            p0 += qv[at * 9 + dd] * rn;
+                            p1 += qv[at * 9 + 3 + dd] * rn;
+                            p2 += qv[at * 9 + 6 + dd] * rn;
+                        }
+                    }
+                }
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            } else {
+                R rold[NP];
+#pragma unroll
+                for (int q = 0; q < NP; ++q) rold[q] = q < n3 ? rs[q * kIonTile + gt] : R(0);
+                /* QG independent accumulation chains; 288 threads leave 168
+                 * registers a thread, which four FP64 chains fit */
+                constexpr int QG = sizeof(R) == 8 ? 4 : 8;
+#pragma unroll 1
+                for (int q0 = 0; q0 < n3c; q0 += QG) {
+                    R acc[QG];
+#pragma unroll
+                    for (int u = 0; u < QG; ++u) {
+                        const int q = q0 + u;
+                        const int at = q / 3, dd = q - 3 * at;
+                        acc[u] = q < n3c ? qm[at * 9 + dd] * e0 + qm[at * 9 + 3 + dd] * e1 + qm[at * 9 + 6 + dd] * e2 : R(0);
+                    }
+#pragma unroll
+                    for (int p = 0; p < NP; p += 2) {
+#pragma unroll
+                        for (int u = 0; u < QG; ++u) {
+                            const R* dr = Dsm + min(q0 + u, NP - 1) * NP + p;
+                            if constexpr (sizeof(R) == 8) {
+                                const double2 d2 = *reinterpret_cast<const double2*>(dr);
+                                acc[u] -= d2.x * rold[p] + d2.y * rold[p + 1];
+                            } else {
+                                acc[u] -= dr[0] * rold[p] + dr[1] * rold[p + 1];
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < QG; ++u) {
+                        const int q = q0 + u;
+                        if (q < n3c) {
+                            const int at = q / 3, dd = q - 3 * at;
+                            const int o = q * kIonTile + gt;
+                            const R vq = vs[o];
+                            const R rn = rs[o] + (vq * dt + R(0.5) * acc[u] * dt * dt);
+                            rs[o] = rn;
+                            vs[o] = vq + acc[u] * dt;
+                            p0 += qv[at * 9 + dd] * rn;
+                            p1 += qv[at * 9 + 3 + dd] * rn;
+                            p2 += qv[at * 9 + 6 + dd] * rn;
+                        }
+                    }
                 }
             }
+            if (n3c) {
+                a.pr[s] = p0;
+                a.pr[ns + s] = p1;
+                a.pr[2 * ns + s] = p2;
+            }
+            /* the updated tile goes back with one tensor store per array;
+             * the stage is free once the store has read it */
+            fence_proxy_async_smem();
+            named_sync(bar_id, kIonTile);
+            if (gt == 0) {
+                const int x = ((int)blockIdx.x + k * (int)gridDim.x) * kIonTile;
+                tma_store_3d(&maps.r, rs, x, 0, 0);
+                tma_store_3d(&maps.v, vs, x, 0, 0);
+                bulk_commit();
+                bulk_wait_read0();
+                atomicMax((int32_t*)consumed, k + 1);
+                mbar_arrive(&empty[st]);
+            }
         }
-        if (n3) {
-            a.pr[s] = p0;
-            a.pr[ns + s] = p1;
-            a.pr[2 * ns + s] = p2;
-        }
-        /* D has been read and A may be rewritten */
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (failed && gt == 0) atomicExch(a.err, 1);
+        if (gt == 0) bulk_wait0(); /* stores complete before the CTA leaves */
     }
-    if (!ok) {
-        if (tid == 0) atomicExch(a.err, 1);
-        /* the MMAs of the abandoned tile may still run: wait for them (again
-         * bounded) before the tensor memory is given back */
-        mbar_wait(bar, phase ^ 1u);
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    if constexpr (P::TC) asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0) {
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(T::COLS));
+    if constexpr (P::TC) {
+        if (warp == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem0),
+                         "r"(P::GROUPS * ion_cols<NP>()));
+        }
     }
 }
 
