@@ -5,7 +5,7 @@ anisotropic grid spacing) and the medium map that generator writes for it.
     python tests/golden/make_medium_golden.py [/path/to/reference]
 
 Runs the reference's generate_medium5.py itself (it needs only numpy); the
-result is committed as golden.npz so that tests never need the reference.
+result is committed as medium_golden.npz so that tests never need the reference.
 """
 import subprocess
 import sys
@@ -42,9 +42,9 @@ def main(ref: Path):
     raw = out.read_bytes()
     shape = np.frombuffer(raw[:12], dtype=np.int32)
     med = np.frombuffer(raw[12:], dtype=np.int32).reshape(shape)
-    np.savez_compressed(HERE / "golden.npz", shape=shape, medium=med)
+    np.savez_compressed(HERE / "medium_golden.npz", shape=shape, medium=med)
     out.unlink()
-    print("wrote", HERE / "golden.npz", shape.tolist(), np.unique(med).tolist())
+    print("wrote", HERE / "medium_golden.npz", shape.tolist(), np.unique(med).tolist())
 
 
 if __name__ == "__main__":

@@ -13,7 +13,7 @@ GOLD = Path(__file__).resolve().parent / "golden" / "medium"
 
 
 def test_shapes_match_the_reference_generator():
-    g = np.load(GOLD / "golden.npz")
+    g = np.load(GOLD / "medium_golden.npz")
     med = geometry.medium_from_cfg((GOLD / "case.cfg").read_text())
     assert med.shape == tuple(g["shape"])
     np.testing.assert_array_equal(med, g["medium"])
@@ -25,7 +25,7 @@ def test_file_format_and_cli(tmp_path):
     raw = out.read_bytes()
     nx, ny, nz = struct.unpack("iii", raw[:12])
     med = np.frombuffer(raw[12:], dtype=np.int32).reshape(nx, ny, nz)
-    np.testing.assert_array_equal(med, np.load(GOLD / "golden.npz")["medium"])
+    np.testing.assert_array_equal(med, np.load(GOLD / "medium_golden.npz")["medium"])
 
 
 def test_no_medium_section_is_vacuum():
