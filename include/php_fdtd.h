@@ -161,6 +161,30 @@ int php_get_step(const php_ctx* ctx, int32_t* t);
  * Registering a probe or a DFT plane afterwards drops them again. */
 int php_prepare(php_ctx* ctx, int32_t nsteps);
 
+/* --- z slabs (several GPUs) ------------------------------------------------ */
+
+/* A context for the planes z0 .. z0+nz_local-1 of the domain `desc`
+ * describes (desc->medium and the sources in global coordinates).  This is
+ * the reference's z decomposition (fdtd.c:2761-2771) with one slab per GPU:
+ * the CPML z profile is the global one, sources outside the slab are
+ * skipped, and every index of the read-out calls is local.  The halo planes
+ * -1 and nz_local hold the neighbours' planes once the caller has copied
+ * them in (see php_halo_planes); at the domain's ends they stay zero. */
+int php_create_slab(const php_desc* desc, int32_t z0, int32_t nz_local, php_ctx** out);
+/* Device addresses of the x, y, z component planes exchanged between
+ * neighbouring slabs (fdtd.c:3120, 3235):
+ *   0  E, plane 0          (sent to the slab below, before the H sweep)
+ *   1  E, halo plane nz    (received from the slab above)
+ *   2  H, plane nz-1       (sent to the slab above, before the E sweep)
+ *   3  H, halo plane -1    (received from the slab below)
+ * Each plane is plane_bytes long (nx padded, times ny, elements). */
+int php_halo_planes(php_ctx* ctx, int32_t which, void** ptrs3, uint64_t* plane_bytes);
+/* Half of one time step, enqueued on the context's stream without a graph:
+ * half 0 = the H sweep; half 1 = the D/E sweep, ion pass, probe and DFT
+ * sample, after which the step counter advances.  A slab's step is
+ * [E halo exchange] half 0 [H halo exchange] half 1. */
+int php_step_half(php_ctx* ctx, int32_t half);
+
 /* --- outputs -------------------------------------------------------------- */
 
 /* One output slice exactly as save_field_slice_parallel writes its data

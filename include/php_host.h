@@ -116,6 +116,20 @@ int php_write_frequency_slice(const char* name, double freq_hz, int32_t freq_ind
                               double source_frequency, double fs, int32_t nsamples,
                               int32_t nx, int32_t ny, const double* re, const double* im);
 
+/* The source frequency frequency_analysis.c takes from a .cfg
+ * (frequency_analysis.c:56-104, 143-148): the frequency= (or wavenumber= x
+ * 0.03e12) of the last `source` line that has one.  Returns PHP_ERR_INPUT
+ * when the file cannot be read or no source line has either. */
+int php_spectra_source_frequency(const char* cfg_path, double* freq_hz);
+
+/* The DFT bins frequency_analysis.c writes (frequency_analysis.c:363-421)
+ * for n_samples slices taken every `interval` steps of dt: the bin nearest
+ * source_frequency and up to four on each side below n_samples / 2.  Fills
+ * up to 9 indices and their frequencies k fs / N; returns the count (0 if
+ * n_samples < 2) and the sampling frequency fs. */
+int32_t php_spectra_bins(int32_t n_samples, int32_t interval, double dt, double source_frequency,
+                         int32_t* index9, double* freq9, double* fs);
+
 #ifdef __cplusplus
 }
 #endif

@@ -121,6 +121,9 @@ DEVICE_SYMBOLS = {
     "php_profile_enable": (_i, [C.c_void_p, _i]),
     "php_profile_read": (_i, [C.c_void_p, _dp, C.POINTER(C.c_int64)]),
     "php_estimate_bytes": (_i, [C.POINTER(Desc), C.POINTER(C.c_uint64)]),
+    "php_create_slab": (_i, [C.POINTER(Desc), _i, _i, C.POINTER(C.c_void_p)]),
+    "php_halo_planes": (_i, [C.c_void_p, _i, C.POINTER(C.c_void_p), C.POINTER(C.c_uint64)]),
+    "php_step_half": (_i, [C.c_void_p, _i]),
     "php_prepare": (_i, [C.c_void_p, _i]),
     "php_server_create": (_i, [C.POINTER(ServerDesc), C.POINTER(C.c_void_p)]),
     "php_server_destroy": (_i, [C.c_void_p]),
@@ -145,6 +148,8 @@ HOST_SYMBOLS = {
     "php_component_from_name": (_i, [C.c_char_p]),
     "php_write_frequency_slice": (_i, [C.c_char_p, _d, _i, _d, _d, _i, _i, _i, _dp, _dp]),
     "php_host_sizeof": (C.c_uint64, [C.c_char_p]),
+    "php_spectra_source_frequency": (_i, [C.c_char_p, C.POINTER(C.c_double)]),
+    "php_spectra_bins": (_i, [_i, _i, _d, _d, C.POINTER(C.c_int32), _dp, _dp]),
 }
 
 _STRUCTS = {"php_desc": Desc, "php_material_desc": MaterialDesc, "php_source_desc": SourceDesc, "php_diag": Diag,

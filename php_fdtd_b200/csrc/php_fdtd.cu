@@ -56,6 +56,8 @@ struct php_ctx {
     int zchunk = 1;
     int n3max = 0, namax_tpl = 0;
     int64_t nslot = 0;           /* pool slots, padded to a multiple of 32 */
+    int z_off = 0, nz_glob = 0;  /* z slab: global index of local plane 0, global nz */
+    int step_part = 3;           /* launches of a step: 1 H sweep, 2 the rest, 3 both */
     int num_sms = 148;
     bool any_ade = false, any_atoms = false;
     cudaStream_t stream = nullptr;
@@ -118,6 +120,8 @@ struct php_ctx {
     /* sweep kernels: TMA plane pipeline (default) or register prefetch */
     bool use_tma = true;
     TmaMaps maps;
+    bool use_x2 = false;         /* FP32: two cells per thread (php_sweeps_x2.cuh) */
+    TmaMaps maps_x2;
     int32_t* err_flag = nullptr;
 
     /* per-kernel timing (php_profile_enable) */
@@ -578,16 +582,32 @@ static void launch_step_t(php_ctx* ctx, int s_local, int& launches)
     StepArgs<R> a = make_args<R>(ctx, s_local);
     dim3 block(kBlockX, kBlockY, 1);
     dim3 grid((ctx->nx + kBlockX - 1) / kBlockX, (ctx->ny + kBlockY - 1) / kBlockY, (ctx->nz + ctx->zchunk - 1) / ctx->zchunk);
-    prof_mark(ctx, s_local, 0, 0);
-    if (ctx->use_tma) h_sweep_tma<R, STRICT><<<grid, block, TmaGeom<R>::H_SMEM, ctx->stream>>>(a, ctx->maps);
-    else h_sweep<R, STRICT><<<grid, block, 0, ctx->stream>>>(a);
-    prof_mark(ctx, s_local, 0, 1);
+    const bool do_h = ctx->step_part & 1, do_e = ctx->step_part & 2;
+    bool x2 = false;
+    if constexpr (sizeof(R) == 4 && !STRICT && NA == 0) x2 = ctx->use_x2;
+    const dim3 grid2((ctx->nx + TmaGeomX2::TX - 1) / TmaGeomX2::TX, grid.y, grid.z);
+    if (do_h) {
+        prof_mark(ctx, s_local, 0, 0);
+        if constexpr (sizeof(R) == 4 && !STRICT && NA == 0) {
+            if (x2) h_sweep_x2<<<grid2, block, TmaGeomX2::H_SMEM, ctx->stream>>>(a, ctx->maps_x2);
+        }
+        if (x2) {
+        } else if (ctx->use_tma) h_sweep_tma<R, STRICT><<<grid, block, TmaGeom<R>::H_SMEM, ctx->stream>>>(a, ctx->maps);
+        else h_sweep<R, STRICT><<<grid, block, 0, ctx->stream>>>(a);
+        prof_mark(ctx, s_local, 0, 1);
+        launches++;
+    }
+    if (!do_e) return;
     prof_mark(ctx, s_local, 1, 0);
-    if (ctx->use_tma)
+    if constexpr (sizeof(R) == 4 && !STRICT && NA == 0) {
+        if (x2) e_sweep_x2<0><<<grid2, block, TmaGeomX2::E_SMEM, ctx->stream>>>(a, ctx->maps_x2);
+    }
+    if (x2) {
+    } else if (ctx->use_tma)
         e_sweep_tma<R, STRICT, NA><<<grid, block, TmaGeom<R>::E_SMEM + a.nmat * sizeof(MatCoef<R>), ctx->stream>>>(a, ctx->maps);
     else e_sweep<R, STRICT, NA><<<grid, block, 0, ctx->stream>>>(a);
     prof_mark(ctx, s_local, 1, 1);
-    launches += 2;
+    launches++;
     if constexpr (!STRICT && NA == 0) {
         if (ctx->ion_split) {
             prof_mark(ctx, s_local, 4, 0);
@@ -704,6 +724,30 @@ static int make_maps(php_ctx* ctx)
         if (!rc) rc = encode_map(ctx, &ctx->maps.d_own[q], base(PHP_DX + q), dt, sizeof(R), nxp, ny, nzh, G::TX, G::TY);
     }
     if (!rc) rc = encode_map(ctx, &ctx->maps.mat, ctx->mat, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, nxp, ny, ctx->nz, G::TX, G::TY);
+    return rc;
+}
+
+/* maps with the 64-cell-wide boxes of php_sweeps_x2.cuh (FP32) */
+static int make_maps_x2(php_ctx* ctx)
+{
+    using G = TmaGeomX2;
+    const CUtensorMapDataType dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    const uint64_t nxp = ctx->nxp, ny = ctx->ny, nzh = ctx->nz + 2;
+    auto base = [&](int q) { return (void*)((char*)ctx->f[q] - (size_t)ctx->plane * sizeof(float)); };
+    int rc = PHP_OK;
+    for (int q = 0; q < 3 && !rc; ++q) {
+        rc = encode_map(ctx, &ctx->maps_x2.e_halo[q], base(PHP_EX + q), dt, 4, nxp, ny, nzh, G::BX, G::BY);
+        if (!rc) rc = encode_map(ctx, &ctx->maps_x2.h_own[q], base(PHP_HX + q), dt, 4, nxp, ny, nzh, G::TX, G::TY);
+        if (!rc) rc = encode_map(ctx, &ctx->maps_x2.h_halo[q], base(PHP_HX + q), dt, 4, nxp, ny, nzh, G::BX, G::BY);
+        if (!rc) rc = encode_map(ctx, &ctx->maps_x2.d_own[q], base(PHP_DX + q), dt, 4, nxp, ny, nzh, G::TX, G::TY);
+    }
+    if (!rc) rc = encode_map(ctx, &ctx->maps_x2.mat, ctx->mat, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, nxp, ny, ctx->nz, G::TX, G::TY);
+    if (!rc) {
+        cudaError_t e = cudaFuncSetAttribute(h_sweep_x2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::H_SMEM);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(e_sweep_x2<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::E_SMEM);
+        if (e != cudaSuccess) return fail(ctx, PHP_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+    }
     return rc;
 }
 
@@ -924,6 +968,7 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
     if (!d.medium) return fail(ctx, PHP_ERR_INPUT, "medium is NULL");
     if (d.num_sources < 0 || (d.num_sources > 0 && !d.sources)) return fail(ctx, PHP_ERR_INPUT, "bad sources");
     ctx->d = d;
+    if (ctx->nz_glob == 0) ctx->nz_glob = d.nz;
     ctx->prec = d.precision;
     ctx->nx = d.nx;
     ctx->ny = d.ny;
@@ -1079,7 +1124,13 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
     AxisD axes[3];
     derive_axis(d, nx, d.dx, false, axes[0]);
     derive_axis(d, ny, d.dy, false, axes[1]);
-    derive_axis(d, nz, d.dz, true, axes[2]);
+    derive_axis(d, ctx->nz_glob, d.dz, true, axes[2]);
+    if (ctx->nz_glob != nz) { /* a z slab: its planes of the global profile */
+        AxisD& z = axes[2];
+        auto cut = [&](auto& v) { v = std::vector<typename std::decay_t<decltype(v)>::value_type>(
+                                      v.begin() + ctx->z_off, v.begin() + ctx->z_off + nz); };
+        cut(z.slot); cut(z.kappa); cut(z.b); cut(z.c); cut(z.kh); cut(z.kd); cut(z.ch); cut(z.cd);
+    }
     if (ctx->prec == PHP_PREC_FP32) rc = upload_tables<float>(ctx, mats, ion_off, ion_coef, axes);
     else rc = upload_tables<double>(ctx, mats, ion_off, ion_coef, axes);
     if (rc) return rc;
@@ -1093,6 +1144,14 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
         rc = ctx->prec == PHP_PREC_FP32 ? make_maps<float>(ctx) : make_maps<double>(ctx);
         if (!rc) rc = pick_step(ctx).prepare(ctx);
         if (rc) return rc;
+        /* FP32 without per-atom state in the E sweep: two cells per thread
+         * on request (PHP_X2=1).  Measured slower than one cell per thread
+         * on B200 (it trades issue slots for latency), so not the default. */
+        const char* x2 = getenv("PHP_X2");
+        if (ctx->prec == PHP_PREC_FP32 && (ctx->namax_tpl == 0 || ctx->ion_split) && x2 && !strcmp(x2, "1")) {
+            if ((rc = make_maps_x2(ctx))) return rc;
+            ctx->use_x2 = true;
+        }
     }
 
     /* per-step inputs, scratch, staging */
@@ -1226,6 +1285,41 @@ static void launch_gather_plane(php_ctx* ctx, int comp, int axis, int pos, bool 
     else gather_plane<R, double><<<296, 256, 0, ctx->stream>>>(f, comp, axis, pos, ctx->nx, ctx->ny, ctx->nz, ctx->nxp, (double*)ctx->scratch);
 }
 
+/* Fills pinned buffer b with the per-step inputs (source values, DFT
+ * sample flags and phasors) of steps t .. t+n-1 and copies it to device
+ * buffer b on the stream. */
+static int stage_step_inputs(php_ctx* ctx, int n, int b)
+{
+    const double dt = ctx->d.dt;
+    /* the copy out of this pinned buffer two chunks ago must be done; the
+     * chunk in between keeps the GPU busy meanwhile */
+    CK(cudaEventSynchronize(ctx->staged[b]));
+    double* h = ctx->step_in_host[b];
+    for (int s = 0; s < n; s++) {
+        const int t = ctx->t + s;
+        double* row = h + (size_t)s * ctx->step_row;
+        const double current_time = t * dt; /* fdtd.c:3117 */
+        for (int q = 0; q < ctx->nsrc_active; q++)
+            row[q] = source_value(&ctx->src[ctx->src_active_index[q]], current_time);
+        for (auto& p : ctx->dft) {
+            const bool take = t >= p.first && ((t - p.first) % p.interval) == 0;
+            row[p.in_off] = take ? 1.0 : 0.0;
+            for (int f = 0; f < p.nfreq; f++) {
+                const double ph = -2.0 * M_PI * p.freq[f] * (t * dt);
+                row[p.in_off + 1 + 2 * f] = take ? cos(ph) : 0.0;
+                row[p.in_off + 2 + 2 * f] = take ? sin(ph) : 0.0;
+            }
+            if (take) p.nsamples++;
+        }
+    }
+    /* the device buffer b was last read by the work of two chunks back,
+     * which precedes this copy on the stream */
+    CK(cudaMemcpyAsync(ctx->step_in_dev[b], h, (size_t)n * ctx->step_row * sizeof(double), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CK(cudaEventRecord(ctx->staged[b], ctx->stream));
+    return PHP_OK;
+}
+
 /* ------------------------------------------------------------- public API */
 
 extern "C" {
@@ -1246,6 +1340,78 @@ int php_create(const php_desc* desc, php_ctx** out)
     return PHP_OK;
 }
 
+int php_create_slab(const php_desc* desc, int32_t z0, int32_t nz_local, php_ctx** out)
+{
+    if (!desc || !out) return fail(nullptr, PHP_ERR_INPUT, "null argument");
+    *out = nullptr;
+    if (!desc->medium || desc->nz < 1 || z0 < 0 || nz_local < 1 || z0 + nz_local > desc->nz)
+        return fail(nullptr, PHP_ERR_INPUT, "slab [%d, %d) outside the grid of %d planes", z0, z0 + nz_local, desc->nz);
+    if (desc->num_sources < 0 || (desc->num_sources > 0 && !desc->sources))
+        return fail(nullptr, PHP_ERR_INPUT, "bad sources");
+    /* the slab's medium and sources in local z */
+    const size_t nx = desc->nx, ny = desc->ny, nzg = desc->nz;
+    std::vector<int32_t> med(nx * ny * (size_t)nz_local);
+    for (size_t i = 0; i < nx; i++)
+        for (size_t j = 0; j < ny; j++)
+            memcpy(&med[(i * ny + j) * nz_local], desc->medium + (i * ny + j) * nzg + z0, sizeof(int32_t) * nz_local);
+    std::vector<php_source_desc> src(desc->sources, desc->sources + std::max(0, desc->num_sources));
+    for (auto& x : src) x.z -= z0; /* sources outside the slab are skipped like those outside the grid */
+    php_desc d = *desc;
+    d.nz = nz_local;
+    d.medium = med.data();
+    d.sources = src.empty() ? nullptr : src.data();
+    php_ctx* ctx = new (std::nothrow) php_ctx();
+    if (!ctx) return fail(nullptr, PHP_ERR_OOM, "host allocation failed");
+    ctx->z_off = z0;
+    ctx->nz_glob = desc->nz;
+    int rc = create_impl(&d, ctx);
+    if (rc) {
+        g_create_error = ctx->err;
+        ctx_free(ctx);
+        return rc;
+    }
+    ctx->d.medium = nullptr; /* the local copies go out of scope */
+    ctx->d.sources = nullptr;
+    *out = ctx;
+    return PHP_OK;
+}
+
+int php_halo_planes(php_ctx* ctx, int32_t which, void** ptrs, uint64_t* plane_bytes)
+{
+    if (!ctx || !ptrs || which < 0 || which > 3) return PHP_ERR_INPUT;
+    /* E plane 0 | E halo above | H top plane | H halo below */
+    const int64_t plane_idx[4] = {0, ctx->nz, ctx->nz - 1, -1};
+    const int first[4] = {PHP_EX, PHP_EX, PHP_HX, PHP_HX};
+    const size_t rs = rsize(ctx->prec);
+    for (int q = 0; q < 3; q++)
+        ptrs[q] = (char*)ctx->f[first[which] + q] + plane_idx[which] * ctx->plane * (int64_t)rs;
+    if (plane_bytes) *plane_bytes = (uint64_t)ctx->plane * rs;
+    return PHP_OK;
+}
+
+int php_step_half(php_ctx* ctx, int32_t half)
+{
+    if (!ctx || (half != 0 && half != 1)) return PHP_ERR_INPUT;
+    ctx->last_launches = 0;
+    int launches = 0;
+    const int b = ctx->chunk_no & 1;
+    if (half == 1) {
+        int rc = stage_step_inputs(ctx, 1, b);
+        if (rc) return rc;
+    }
+    ctx->step_in = ctx->step_in_dev[b];
+    ctx->step_part = half == 0 ? 1 : 2;
+    pick_step(ctx).launch(ctx, 0, launches);
+    ctx->step_part = 3;
+    CK(cudaGetLastError());
+    if (half == 1) {
+        ctx->chunk_no++;
+        ctx->t++;
+    }
+    ctx->last_launches = launches;
+    return PHP_OK;
+}
+
 int php_destroy(php_ctx* ctx)
 {
     ctx_free(ctx);
@@ -1263,38 +1429,15 @@ int php_step(php_ctx* ctx, int32_t nsteps)
     if (!ctx) return PHP_ERR_INPUT;
     if (nsteps < 0) return fail(ctx, PHP_ERR_INPUT, "negative step count");
     ctx->last_launches = 0;
-    const double dt = ctx->d.dt;
     while (nsteps > 0) {
         const int n = std::min(nsteps, kMaxChunk);
         const int b = ctx->chunk_no & 1;
         /* the copy out of this pinned buffer two chunks ago must be done;
          * the chunk in between keeps the GPU busy meanwhile */
-        CK(cudaEventSynchronize(ctx->staged[b]));
-        double* h = ctx->step_in_host[b];
-        for (int s = 0; s < n; s++) {
-            const int t = ctx->t + s;
-            double* row = h + (size_t)s * ctx->step_row;
-            const double current_time = t * dt; /* fdtd.c:3117 */
-            for (int q = 0; q < ctx->nsrc_active; q++)
-                row[q] = source_value(&ctx->src[ctx->src_active_index[q]], current_time);
-            for (auto& p : ctx->dft) {
-                const bool take = t >= p.first && ((t - p.first) % p.interval) == 0;
-                row[p.in_off] = take ? 1.0 : 0.0;
-                for (int f = 0; f < p.nfreq; f++) {
-                    const double ph = -2.0 * M_PI * p.freq[f] * (t * dt);
-                    row[p.in_off + 1 + 2 * f] = take ? cos(ph) : 0.0;
-                    row[p.in_off + 2 + 2 * f] = take ? sin(ph) : 0.0;
-                }
-                if (take) p.nsamples++;
-            }
-        }
-        /* the device buffer b was last read by the graph two chunks back,
-         * which precedes this copy on the stream */
-        CK(cudaMemcpyAsync(ctx->step_in_dev[b], h, (size_t)n * ctx->step_row * sizeof(double), cudaMemcpyHostToDevice,
-                           ctx->stream));
-        CK(cudaEventRecord(ctx->staged[b], ctx->stream));
+        int rc = stage_step_inputs(ctx, n, b);
+        if (rc) return rc;
         cudaGraphExec_t g;
-        int rc = ensure_graph(ctx, n, b, &g);
+        rc = ensure_graph(ctx, n, b, &g);
         if (rc) return rc;
         CK(cudaGraphLaunch(g, ctx->stream));
         ctx->chunk_no++;

@@ -565,19 +565,18 @@ __device__ __forceinline__ void e_update(const StepArgs<R>& a, const MatCoef<R>&
 
 /* One cell of the fused sweep once its H values are known: D update on
  * the interior with the lossy eps'' term (fdtd.c:3238-3356), the sources of
- * this step (fdtd.c:3363-3396), D -> E / ADE / ions (fdtd.c:3404-3528); D and E
- * are stored to global memory. */
+ * this step (fdtd.c:3363-3396), D -> E / ADE / ions (fdtd.c:3404-3528).  The
+ * new D and E come back in dx..dz and ex_out..ez_out; the caller stores
+ * them (e_cell below, or the two-cell sweep with paired stores). */
 template <typename R, bool STRICT, int NAMAX>
-__device__ __forceinline__ void e_cell(const StepArgs<R>& a, int i, int j, int k, int c, bool interior, int sx, int sy,
-                                       R hx0, R hy0, R hz0, R hxk, R hyk, R hz_jm, R hx_jm, R hz_im, R hy_im, R dx, R dy,
-                                       R dz, int mid, const MatCoef<R>* mcs, const CellPsi<R>* pre)
+__device__ __forceinline__ void e_cell_values(const StepArgs<R>& a, int i, int j, int k, int c, bool interior, int sx,
+                                              int sy, R hx0, R hy0, R hz0, R hxk, R hyk, R hz_jm, R hx_jm, R hz_im,
+                                              R hy_im, R& dx, R& dy, R& dz, int mid, const MatCoef<R>* mcs,
+                                              const CellPsi<R>* pre, R& ex_out, R& ey_out, R& ez_out)
 {
-    R* __restrict__ dxp = a.f.dx;
-    R* __restrict__ dyp = a.f.dy;
-    R* __restrict__ dzp = a.f.dz;
-    R* __restrict__ exp_ = a.f.ex;
-    R* __restrict__ eyp = a.f.ey;
-    R* __restrict__ ezp = a.f.ez;
+    const R* __restrict__ exp_ = a.f.ex;
+    const R* __restrict__ eyp = a.f.ey;
+    const R* __restrict__ ezp = a.f.ez;
     /* mcs: the block's shared-memory copy of the first kSmemMats records */
     const MatCoef<R>& m = (mcs && mid < a.nmat) ? mcs[mid] : a.mc[mid];
     const int flags = m.flags;
@@ -630,13 +629,27 @@ __device__ __forceinline__ void e_cell(const StepArgs<R>& a, int i, int j, int k
         dy += iy;
         dz += iz;
     }
-    dxp[c] = dx;
-    dyp[c] = dy;
-    dzp[c] = dz;
     e_update<R, STRICT, NAMAX>(a, m, c, dx, dy, dz, ix, iy, iz, ex, ey, ez);
-    exp_[c] = ex;
-    eyp[c] = ey;
-    ezp[c] = ez;
+    ex_out = ex;
+    ey_out = ey;
+    ez_out = ez;
+}
+
+/* e_cell_values with D and E stored to global memory */
+template <typename R, bool STRICT, int NAMAX>
+__device__ __forceinline__ void e_cell(const StepArgs<R>& a, int i, int j, int k, int c, bool interior, int sx, int sy,
+                                       R hx0, R hy0, R hz0, R hxk, R hyk, R hz_jm, R hx_jm, R hz_im, R hy_im, R dx, R dy,
+                                       R dz, int mid, const MatCoef<R>* mcs, const CellPsi<R>* pre)
+{
+    R ex, ey, ez;
+    e_cell_values<R, STRICT, NAMAX>(a, i, j, k, c, interior, sx, sy, hx0, hy0, hz0, hxk, hyk, hz_jm, hx_jm, hz_im, hy_im,
+                                    dx, dy, dz, mid, mcs, pre, ex, ey, ez);
+    a.f.dx[c] = dx;
+    a.f.dy[c] = dy;
+    a.f.dz[c] = dz;
+    a.f.ex[c] = ex;
+    a.f.ey[c] = ey;
+    a.f.ez[c] = ez;
 }
 
 template <typename R>

@@ -2,7 +2,7 @@
  * fdtd_b200 -- drop-in replacement for PhP_FDTD's solver executable
  * (fdtd.x, fdtd.c:2075-4083) on one B200.
  *
- *   fdtd_b200 <config.cfg> [fp64|fp64-strict|fp32]
+ *   fdtd_b200 <config.cfg> [fp64|fp64-strict|fp32] [--spectra]
  *
  * Reads the same .cfg, medium_map.bin and material files, prints the same
  * progress lines and writes the same output files as a single-rank run of
@@ -11,6 +11,11 @@
  *   monitor_point.dat (monitor_output_file)  every step
  *   full_monitor.dat                         every output_interval steps
  *   source.txt                               every output_interval steps
+ * and with --spectra, at the end, the frequency_slice_*.txt files that the
+ * reference's post-processor (frequency_analysis.c) derives from the z slices:
+ * the same bins, normalisation, columns and central crop, accumulated on the
+ * device at the output steps from the float32 slice values instead of an FFT
+ * over the slice files.
  * The time loop (fdtd.c:3116-3884) runs on the GPU through libphpfdtd; this
  * file is the host loop around it, with the reference's output cadence and
  * index conventions (monitor and z-slice fields read at k+1, atoms at k,
@@ -88,11 +93,16 @@ int main(int argc, char** argv)
 {
     printf("FDTD (B200) running on 1 GPU\n");
     if (argc < 2) {
-        printf("Usage: %s <config_file.cfg> [fp64|fp64-strict|fp32]\n", argv[0]);
+        printf("Usage: %s <config_file.cfg> [fp64|fp64-strict|fp32] [--spectra]\n", argv[0]);
         return 1;
     }
     int precision = PHP_PREC_FP64;
-    const char* pa = argc > 2 ? argv[2] : getenv("PHP_PRECISION");
+    int spectra = 0;
+    const char* pa = getenv("PHP_PRECISION");
+    for (int a = 2; a < argc; a++) {
+        if (!strcmp(argv[a], "--spectra")) spectra = 1;
+        else pa = argv[a];
+    }
     if (pa) {
         if (!strcmp(pa, "fp64-strict")) precision = PHP_PREC_FP64_STRICT;
         else if (!strcmp(pa, "fp32")) precision = PHP_PREC_FP32;
@@ -152,6 +162,27 @@ int main(int argc, char** argv)
     }
     free(medium);
     medium = NULL;
+
+    /* running DFT of the output slice at the post-processor's bins
+     * (frequency_analysis.c:363-421): samples at t % output_interval == 0,
+     * float32 like the slice files, z slices of a field component */
+    int spectra_id = -1, spectra_n = 0, spectra_count = 0;
+    int32_t spectra_index[9];
+    double spectra_freq[9], spectra_fs = 0.0, spectra_src = 0.0;
+    const int spectra_comp = php_component_from_name(cfg->output_component);
+    if (spectra) {
+        spectra_n = (cfg->tsteps - 1) / cfg->output_interval + 1;
+        if (cfg->output_slice_axis != 'z' || spectra_comp < 0 || spectra_comp > PHP_HZ)
+            fprintf(stderr, "--spectra: needs a z slice of a field component; skipped\n");
+        else if (php_spectra_source_frequency(argv[1], &spectra_src))
+            fprintf(stderr, "--spectra: no source frequency in %s; skipped\n", argv[1]);
+        else if ((spectra_count = php_spectra_bins(spectra_n, cfg->output_interval, cfg->dt, spectra_src, spectra_index,
+                                                   spectra_freq, &spectra_fs)) > 0) {
+            if ((rc = php_dft_add(ctx, spectra_comp, cfg->output_slice_position + 1, 0, cfg->output_interval,
+                                  spectra_count, spectra_freq, 1, &spectra_id)))
+                return device_fail(ctx, "php_dft_add", rc);
+        }
+    }
 
     FILE* source_file = fopen("source.txt", "w");
     if (!source_file) fprintf(stderr, "Error opening source.txt for writing\n");
@@ -261,6 +292,29 @@ int main(int argc, char** argv)
         t = next + 1;
     }
     php_sync(ctx);
+    if (spectra_id >= 0 && exit_code == 0) {
+        double* acc = (double*)malloc(sizeof(double) * 2 * (size_t)spectra_count * nx * ny);
+        double* re = (double*)malloc(sizeof(double) * (size_t)nx * ny);
+        double* im = (double*)malloc(sizeof(double) * (size_t)nx * ny);
+        int32_t ns = 0;
+        if (acc && re && im && php_dft_read(ctx, spectra_id, acc, &ns) == PHP_OK) {
+            for (int f = 0; f < spectra_count; f++) {
+                for (size_t q = 0; q < (size_t)nx * ny; q++) {
+                    re[q] = acc[2 * ((size_t)f * nx * ny + q)] / ns;
+                    im[q] = acc[2 * ((size_t)f * nx * ny + q) + 1] / ns;
+                }
+                char name[256];
+                snprintf(name, sizeof(name), "frequency_slice_%d_%.3eHz_%.3ecm-1.txt", spectra_index[f], spectra_freq[f],
+                         spectra_freq[f] / 0.03e12);
+                php_write_frequency_slice(name, spectra_freq[f], spectra_index[f], spectra_src, spectra_fs, ns, nx, ny, re,
+                                          im);
+                printf("  Results saved to %s\n", name);
+            }
+        }
+        free(acc);
+        free(re);
+        free(im);
+    }
     if (source_file) fclose(source_file);
     if (monitor_file) {
         fclose(monitor_file);

@@ -812,6 +812,73 @@ int php_write_frequency_slice(const char* name, double freq_hz, int32_t freq_ind
     return PHP_OK;
 }
 
+int php_spectra_source_frequency(const char* cfg_path, double* freq_hz)
+{
+    if (!cfg_path || !freq_hz) return PHP_ERR_INPUT;
+    FILE* f = fopen(cfg_path, "r");
+    if (!f) return PHP_ERR_INPUT;
+    char line[256];
+    double found = 0.0;
+    while (fgets(line, sizeof(line), f)) {
+        line[strcspn(line, "\n")] = 0;
+        if (line[0] == '#' || strstr(line, "source") != line) continue;
+        double fr = 0.0, wn = 0.0;
+        int has_f = 0, has_w = 0;
+        char* save = NULL;
+        for (char* tok = strtok_r(line, ",", &save); tok; tok = strtok_r(NULL, ",", &save)) {
+            char* eq = strchr(tok, '=');
+            if (!eq) continue;
+            if (strstr(tok, "frequency")) {
+                fr = atof(eq + 1);
+                has_f = 1;
+            } else if (strstr(tok, "wavenumber")) {
+                wn = atof(eq + 1);
+                has_w = 1;
+            }
+        }
+        if (has_f && has_w) {
+            fclose(f);
+            return PHP_ERR_INPUT;
+        }
+        if (has_w) fr = wn * 0.03e12, has_f = 1;
+        if (has_f) found = fr;
+    }
+    fclose(f);
+    if (!(found > 0.0)) return PHP_ERR_INPUT;
+    *freq_hz = found;
+    return PHP_OK;
+}
+
+int32_t php_spectra_bins(int32_t n, int32_t interval, double dt, double source_frequency, int32_t* index9,
+                         double* freq9, double* fs_out)
+{
+    if (n < 2 || interval < 1 || !index9 || !freq9) return 0;
+    /* sample times as the analysis reads them from the slice file names */
+    const double t_first = 0.0 * dt, t_last = (double)((int64_t)(n - 1) * interval) * dt;
+    const double T = t_last - t_first;
+    const double fs = 1.0 / (T / (n - 1));
+    int target = -1;
+    double best = 1e100;
+    for (int i = 0; i < n / 2; i++) {
+        const double d = fabs(i * fs / n - source_frequency);
+        if (d < best) {
+            best = d;
+            target = i;
+        }
+    }
+    int32_t count = 0;
+    for (int off = -4; off <= 4 && count < 9; off++) {
+        const int idx = target + off;
+        if (idx >= 0 && idx < n / 2) {
+            index9[count] = idx;
+            freq9[count] = idx * fs / n;
+            count++;
+        }
+    }
+    if (fs_out) *fs_out = fs;
+    return count;
+}
+
 uint64_t php_host_sizeof(const char* n)
 {
     if (!n) return 0;
