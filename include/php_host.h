@@ -116,11 +116,13 @@ int php_write_frequency_slice(const char* name, double freq_hz, int32_t freq_ind
                               double source_frequency, double fs, int32_t nsamples,
                               int32_t nx, int32_t ny, const double* re, const double* im);
 
-/* The source frequency frequency_analysis.c takes from a .cfg
- * (frequency_analysis.c:56-104, 143-148): the frequency= (or wavenumber= x
- * 0.03e12) of the last `source` line that has one.  Returns PHP_ERR_INPUT
- * when the file cannot be read or no source line has either. */
-int php_spectra_source_frequency(const char* cfg_path, double* freq_hz);
+/* What frequency_analysis.c takes from a .cfg (frequency_analysis.c:56-148):
+ * the frequency= (or wavenumber= x 0.03e12) of the last `source` line that
+ * has one, and the explicit `dt` line (*dt = -1 when there is none; the
+ * solver itself may have lowered dt to the Courant limit, fdtd.c:1910).
+ * Returns PHP_ERR_INPUT when the file cannot be read or no source line has
+ * a frequency. */
+int php_spectra_config(const char* cfg_path, double* freq_hz, double* dt);
 
 /* The DFT bins frequency_analysis.c writes (frequency_analysis.c:363-421)
  * for n_samples slices taken every `interval` steps of dt: the bin nearest

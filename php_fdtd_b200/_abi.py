@@ -148,7 +148,7 @@ HOST_SYMBOLS = {
     "php_component_from_name": (_i, [C.c_char_p]),
     "php_write_frequency_slice": (_i, [C.c_char_p, _d, _i, _d, _d, _i, _i, _i, _dp, _dp]),
     "php_host_sizeof": (C.c_uint64, [C.c_char_p]),
-    "php_spectra_source_frequency": (_i, [C.c_char_p, C.POINTER(C.c_double)]),
+    "php_spectra_config": (_i, [C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "php_spectra_bins": (_i, [_i, _i, _d, _d, C.POINTER(C.c_int32), _dp, _dp]),
 }
 

@@ -120,8 +120,6 @@ struct php_ctx {
     /* sweep kernels: TMA plane pipeline (default) or register prefetch */
     bool use_tma = true;
     TmaMaps maps;
-    bool use_x2 = false;         /* FP32: two cells per thread (php_sweeps_x2.cuh) */
-    TmaMaps maps_x2;
     int32_t* err_flag = nullptr;
 
     /* per-kernel timing (php_profile_enable) */
@@ -583,27 +581,16 @@ static void launch_step_t(php_ctx* ctx, int s_local, int& launches)
     dim3 block(kBlockX, kBlockY, 1);
     dim3 grid((ctx->nx + kBlockX - 1) / kBlockX, (ctx->ny + kBlockY - 1) / kBlockY, (ctx->nz + ctx->zchunk - 1) / ctx->zchunk);
     const bool do_h = ctx->step_part & 1, do_e = ctx->step_part & 2;
-    bool x2 = false;
-    if constexpr (sizeof(R) == 4 && !STRICT && NA == 0) x2 = ctx->use_x2;
-    const dim3 grid2((ctx->nx + TmaGeomX2::TX - 1) / TmaGeomX2::TX, grid.y, grid.z);
     if (do_h) {
         prof_mark(ctx, s_local, 0, 0);
-        if constexpr (sizeof(R) == 4 && !STRICT && NA == 0) {
-            if (x2) h_sweep_x2<<<grid2, block, TmaGeomX2::H_SMEM, ctx->stream>>>(a, ctx->maps_x2);
-        }
-        if (x2) {
-        } else if (ctx->use_tma) h_sweep_tma<R, STRICT><<<grid, block, TmaGeom<R>::H_SMEM, ctx->stream>>>(a, ctx->maps);
+        if (ctx->use_tma) h_sweep_tma<R, STRICT><<<grid, block, TmaGeom<R>::H_SMEM, ctx->stream>>>(a, ctx->maps);
         else h_sweep<R, STRICT><<<grid, block, 0, ctx->stream>>>(a);
         prof_mark(ctx, s_local, 0, 1);
         launches++;
     }
     if (!do_e) return;
     prof_mark(ctx, s_local, 1, 0);
-    if constexpr (sizeof(R) == 4 && !STRICT && NA == 0) {
-        if (x2) e_sweep_x2<0><<<grid2, block, TmaGeomX2::E_SMEM, ctx->stream>>>(a, ctx->maps_x2);
-    }
-    if (x2) {
-    } else if (ctx->use_tma)
+    if (ctx->use_tma)
         e_sweep_tma<R, STRICT, NA><<<grid, block, TmaGeom<R>::E_SMEM + a.nmat * sizeof(MatCoef<R>), ctx->stream>>>(a, ctx->maps);
     else e_sweep<R, STRICT, NA><<<grid, block, 0, ctx->stream>>>(a);
     prof_mark(ctx, s_local, 1, 1);
@@ -724,30 +711,6 @@ static int make_maps(php_ctx* ctx)
         if (!rc) rc = encode_map(ctx, &ctx->maps.d_own[q], base(PHP_DX + q), dt, sizeof(R), nxp, ny, nzh, G::TX, G::TY);
     }
     if (!rc) rc = encode_map(ctx, &ctx->maps.mat, ctx->mat, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, nxp, ny, ctx->nz, G::TX, G::TY);
-    return rc;
-}
-
-/* maps with the 64-cell-wide boxes of php_sweeps_x2.cuh (FP32) */
-static int make_maps_x2(php_ctx* ctx)
-{
-    using G = TmaGeomX2;
-    const CUtensorMapDataType dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-    const uint64_t nxp = ctx->nxp, ny = ctx->ny, nzh = ctx->nz + 2;
-    auto base = [&](int q) { return (void*)((char*)ctx->f[q] - (size_t)ctx->plane * sizeof(float)); };
-    int rc = PHP_OK;
-    for (int q = 0; q < 3 && !rc; ++q) {
-        rc = encode_map(ctx, &ctx->maps_x2.e_halo[q], base(PHP_EX + q), dt, 4, nxp, ny, nzh, G::BX, G::BY);
-        if (!rc) rc = encode_map(ctx, &ctx->maps_x2.h_own[q], base(PHP_HX + q), dt, 4, nxp, ny, nzh, G::TX, G::TY);
-        if (!rc) rc = encode_map(ctx, &ctx->maps_x2.h_halo[q], base(PHP_HX + q), dt, 4, nxp, ny, nzh, G::BX, G::BY);
-        if (!rc) rc = encode_map(ctx, &ctx->maps_x2.d_own[q], base(PHP_DX + q), dt, 4, nxp, ny, nzh, G::TX, G::TY);
-    }
-    if (!rc) rc = encode_map(ctx, &ctx->maps_x2.mat, ctx->mat, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, nxp, ny, ctx->nz, G::TX, G::TY);
-    if (!rc) {
-        cudaError_t e = cudaFuncSetAttribute(h_sweep_x2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::H_SMEM);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(e_sweep_x2<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::E_SMEM);
-        if (e != cudaSuccess) return fail(ctx, PHP_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
-    }
     return rc;
 }
 
@@ -1144,14 +1107,6 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
         rc = ctx->prec == PHP_PREC_FP32 ? make_maps<float>(ctx) : make_maps<double>(ctx);
         if (!rc) rc = pick_step(ctx).prepare(ctx);
         if (rc) return rc;
-        /* FP32 without per-atom state in the E sweep: two cells per thread
-         * on request (PHP_X2=1).  Measured slower than one cell per thread
-         * on B200 (it trades issue slots for latency), so not the default. */
-        const char* x2 = getenv("PHP_X2");
-        if (ctx->prec == PHP_PREC_FP32 && (ctx->namax_tpl == 0 || ctx->ion_split) && x2 && !strcmp(x2, "1")) {
-            if ((rc = make_maps_x2(ctx))) return rc;
-            ctx->use_x2 = true;
-        }
     }
 
     /* per-step inputs, scratch, staging */

@@ -336,4 +336,3 @@ __global__ void __launch_bounds__(256) diag_pass2(const DiagPartial* scratch, in
 #include "php_sweeps.cuh"
 #include "php_sweeps_tma.cuh"
 #include "php_ions.cuh"
-#include "php_sweeps_x2.cuh"

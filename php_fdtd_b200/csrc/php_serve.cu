@@ -107,6 +107,10 @@ namespace {
 bool build_job(php_server* s, Job* j)
 {
     j->desc.device = s->d.device;
+    /* the device is shared by the running jobs: a small grid keeps 8-plane z
+     * chunks (fewer halo re-reads) instead of splitting its z range until its
+     * own blocks fill the GPU */
+    if (j->desc.z_chunk <= 0) j->desc.z_chunk = 8;
     int rc = php_create(&j->desc, &j->ctx);
     if (rc) {
         set_error(j, rc, php_last_error(nullptr));

@@ -364,6 +364,26 @@ __device__ __forceinline__ void d_update(const StepArgs<R>& a, int i, int j, int
     }
 }
 
+/* bytes of r (and again of v) per cell up to which the fused sweep holds a
+ * cell's ion state in registers: 6 FP32 coordinates (two atoms) fit the
+ * 64-register budget of the FP32 sweep without spills, FP64 ones do not */
+constexpr int kIonRegBytes = 24;
+
+/* f(q) for q = 0 .. n3-1 in order; with UNR fully unrolled over the bound
+ * QN (predicated), so that arrays indexed by q stay in registers */
+template <int QN, bool UNR, typename F>
+__device__ __forceinline__ void for_atoms(int n3, F&& f)
+{
+    if constexpr (UNR) {
+#pragma unroll
+        for (int q = 0; q < QN; ++q)
+            if (q < n3) f(q);
+    } else {
+#pragma unroll 6
+        for (int q = 0; q < n3; ++q) f(q);
+    }
+}
+
 /* D -> E, ADE and ions for one cell (fdtd.c:3404-3528).  ex..ez hold E^n on
  * entry (lab frame) and E^{n+1} on return; dx..dz are D^{n+1}; ix..iz are
  * D^{n+1} - D^n as summed before rounding into D (FP32 only). */
@@ -385,17 +405,36 @@ __device__ __forceinline__ void e_update(const StepArgs<R>& a, const MatCoef<R>&
     if (flags & (kAde | kAtoms)) slot = a.slot[c];
     const int64_t ns = a.nslot;
 
-    /* P_ion = QeZV . r^n in the crystal frame (fdtd.c:3418-3427) */
+    /* P_ion = QeZV . r^n in the crystal frame (fdtd.c:3418-3427).  With
+     * few atoms (VREG) r and v of the cell sit in registers and all 2 x 3N
+     * loads are issued together here. */
+    constexpr int QN = NAMAX > 0 ? 3 * NAMAX : 1;
+    constexpr bool VREG = QN * (int)sizeof(R) <= kIonRegBytes;
     R pr0 = R(0), pr1 = R(0), pr2 = R(0);
-    R rold[NAMAX > 0 ? 3 * NAMAX : 1];
+    R rold[QN];
+    R vold[VREG ? QN : 1];
     const int n3 = (NAMAX > 0 && (flags & kAtoms)) ? 3 * m.natom : 0;
     if constexpr (NAMAX > 0) {
         if (n3) {
             const R* qv = a.ion_coef + m.ion_off;
-#pragma unroll 6
-            for (int q = 0; q < n3; ++q) {
-                const R rq = a.r[(int64_t)q * ns + slot];
-                rold[q] = rq;
+            if constexpr (VREG) {
+#pragma unroll
+                for (int q = 0; q < QN; ++q)
+                    if (q < n3) {
+                        rold[q] = a.r[(int64_t)q * ns + slot];
+                        vold[q] = a.v[(int64_t)q * ns + slot];
+                    }
+            }
+            for_atoms<QN, VREG>(n3, [&](int q) {
+                R rq;
+                if constexpr (VREG) {
+                    rq = rold[q];
+                } else {
+                    rq = a.r[(int64_t)q * ns + slot];
+                    rold[q] = rq;
+                    /* v is read after E^{n+1}: bring it into L1 now */
+                    asm volatile("prefetch.global.L1 [%0];" ::"l"(a.v + (int64_t)q * ns + slot));
+                }
                 const int at = q / 3, d = q - 3 * at;
                 const R q0 = ldg(qv + at * 9 + 0 * 3 + d);
                 const R q1 = ldg(qv + at * 9 + 1 * 3 + d);
@@ -409,7 +448,7 @@ __device__ __forceinline__ void e_update(const StepArgs<R>& a, const MatCoef<R>&
                     pr1 += q1 * rq;
                     pr2 += q2 * rq;
                 }
-            }
+            });
         }
     }
 
@@ -529,7 +568,7 @@ __device__ __forceinline__ void e_update(const StepArgs<R>& a, const MatCoef<R>&
             const R* qm = a.ion_coef + m.ion_off + 3 * n3;
             const R* dmm = qm + 3 * n3;
             const R dt = R(a.dt);
-            for (int q = 0; q < n3; ++q) {
+            for_atoms<QN, VREG>(n3, [&](int q) {
                 const int at = q / 3, d = q - 3 * at;
                 const R m0 = ldg(qm + at * 9 + 0 * 3 + d);
                 const R m1 = ldg(qm + at * 9 + 1 * 3 + d);
@@ -538,14 +577,15 @@ __device__ __forceinline__ void e_update(const StepArgs<R>& a, const MatCoef<R>&
                 R acc;
                 if constexpr (STRICT) {
                     acc = SOp::add(SOp::add(SOp::mul(m0, na), SOp::mul(m1, nb)), SOp::mul(m2, nc));
-                    for (int p = 0; p < n3; ++p) acc = SOp::sub(acc, SOp::mul(ldg(row + p), rold[p]));
+                    for_atoms<QN, VREG>(n3, [&](int p) { acc = SOp::sub(acc, SOp::mul(ldg(row + p), rold[p])); });
                 } else {
                     acc = m0 * na + m1 * nb + m2 * nc;
-#pragma unroll 6
-                    for (int p = 0; p < n3; ++p) acc -= ldg(row + p) * rold[p];
+                    for_atoms<QN, VREG>(n3, [&](int p) { acc -= ldg(row + p) * rold[p]; });
                 }
                 const int64_t o = (int64_t)q * ns + slot;
-                const R vq = a.v[o];
+                R vq;
+                if constexpr (VREG) vq = vold[q];
+                else vq = a.v[o];
                 if constexpr (STRICT) {
                     a.r[o] = SOp::add(rold[q], SOp::add(SOp::mul(vq, a.dt), SOp::mul(SOp::mul(SOp::mul(0.5, acc), a.dt), a.dt)));
                     a.v[o] = SOp::add(vq, SOp::mul(acc, a.dt));
@@ -553,7 +593,7 @@ __device__ __forceinline__ void e_update(const StepArgs<R>& a, const MatCoef<R>&
                     a.r[o] = rold[q] + (vq * dt + R(0.5) * acc * dt * dt);
                     a.v[o] = vq + acc * dt;
                 }
-            }
+            });
         }
     }
 

@@ -51,6 +51,10 @@ constexpr uint32_t kWaitLimit = 1u << 24;
 #ifndef PHP_PSI_EARLY_H32
 #define PHP_PSI_EARLY_H32 0
 #endif
+/* resident blocks the fused sweep is compiled for (register budget) */
+#ifndef PHP_E_MINBLOCKS32
+#define PHP_E_MINBLOCKS32 4
+#endif
 #ifndef PHP_PSI_EARLY_E
 #define PHP_PSI_EARLY_E 1
 #endif
@@ -331,7 +335,7 @@ __global__ void __launch_bounds__(kBlockX * kBlockY) h_sweep_tma(const __grid_co
 /* fdtd.c:3238-3528 fused, as e_sweep, with H, D and the material ids
  * streamed through the stage ring. */
 template <typename R, bool STRICT, int NAMAX>
-__global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : PHP_E_MINBLOCKS))
+__global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) == 4 ? PHP_E_MINBLOCKS32 : PHP_E_MINBLOCKS))
     e_sweep_tma(const __grid_constant__ StepArgs<R> a, const __grid_constant__ TmaMaps tm)
 {
     using G = TmaGeom<R>;

@@ -168,18 +168,29 @@ int main(int argc, char** argv)
      * float32 like the slice files, z slices of a field component */
     int spectra_id = -1, spectra_n = 0, spectra_count = 0;
     int32_t spectra_index[9];
-    double spectra_freq[9], spectra_fs = 0.0, spectra_src = 0.0;
+    double spectra_freq[9], spectra_fs = 0.0, spectra_src = 0.0, spectra_dt = -1.0;
     const int spectra_comp = php_component_from_name(cfg->output_component);
     if (spectra) {
         spectra_n = (cfg->tsteps - 1) / cfg->output_interval + 1;
         if (cfg->output_slice_axis != 'z' || spectra_comp < 0 || spectra_comp > PHP_HZ)
             fprintf(stderr, "--spectra: needs a z slice of a field component; skipped\n");
-        else if (php_spectra_source_frequency(argv[1], &spectra_src))
+        else if (php_spectra_config(argv[1], &spectra_src, &spectra_dt))
             fprintf(stderr, "--spectra: no source frequency in %s; skipped\n", argv[1]);
-        else if ((spectra_count = php_spectra_bins(spectra_n, cfg->output_interval, cfg->dt, spectra_src, spectra_index,
-                                                   spectra_freq, &spectra_fs)) > 0) {
-            if ((rc = php_dft_add(ctx, spectra_comp, cfg->output_slice_position + 1, 0, cfg->output_interval,
-                                  spectra_count, spectra_freq, 1, &spectra_id)))
+        else {
+            /* bins and their labels as the post-processor computes them from
+             * the .cfg's dt line (the solver's dt when there is none) ... */
+            const double label_dt = spectra_dt > 0 ? spectra_dt : cfg->dt;
+            spectra_count = php_spectra_bins(spectra_n, cfg->output_interval, label_dt, spectra_src, spectra_index,
+                                             spectra_freq, &spectra_fs);
+            /* ... and sampled on the solver's own time base, so that bin k
+             * is exactly exp(-2 pi i k n / N) over the N output steps */
+            double fs_solver = 0.0, f_solver[9];
+            int32_t idx_solver[9];
+            php_spectra_bins(spectra_n, cfg->output_interval, cfg->dt, spectra_src, idx_solver, f_solver, &fs_solver);
+            for (int f = 0; f < spectra_count; f++) f_solver[f] = spectra_index[f] * fs_solver / spectra_n;
+            if (spectra_count > 0 &&
+                (rc = php_dft_add(ctx, spectra_comp, cfg->output_slice_position + 1, 0, cfg->output_interval,
+                                  spectra_count, f_solver, 1, &spectra_id)))
                 return device_fail(ctx, "php_dft_add", rc);
         }
     }

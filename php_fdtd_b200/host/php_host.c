@@ -812,16 +812,23 @@ int php_write_frequency_slice(const char* name, double freq_hz, int32_t freq_ind
     return PHP_OK;
 }
 
-int php_spectra_source_frequency(const char* cfg_path, double* freq_hz)
+int php_spectra_config(const char* cfg_path, double* freq_hz, double* dt)
 {
-    if (!cfg_path || !freq_hz) return PHP_ERR_INPUT;
+    if (!cfg_path || !freq_hz || !dt) return PHP_ERR_INPUT;
     FILE* f = fopen(cfg_path, "r");
     if (!f) return PHP_ERR_INPUT;
     char line[256];
     double found = 0.0;
+    *dt = -1.0;
     while (fgets(line, sizeof(line), f)) {
         line[strcspn(line, "\n")] = 0;
-        if (line[0] == '#' || strstr(line, "source") != line) continue;
+        if (line[0] == '#') continue;
+        if (strstr(line, "dt") == line) {
+            const char* eq = strchr(line, '=');
+            if (eq) *dt = atof(eq + 1);
+            continue;
+        }
+        if (strstr(line, "source") != line) continue;
         double fr = 0.0, wn = 0.0;
         int has_f = 0, has_w = 0;
         char* save = NULL;

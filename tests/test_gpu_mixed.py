@@ -60,27 +60,3 @@ def test_fp32_fields_and_nearfield_within_bounds():
         assert scale > 0
         np.testing.assert_allclose(s32[key], s64[key], rtol=0, atol=1e-3 * scale, err_msg=key)
 
-
-def test_two_cell_fp32_sweeps_match_one_cell(golden_case):
-    """PHP_X2=1 (two cells per thread) against the default FP32 sweeps."""
-    import os
-    import harness as H
-    from php_fdtd_b200 import Config
-    for name in ("aniso_lossy", "lossy_rot", "ade_metal"):
-        with H.chdir(golden_case(name)):
-            cfg = Config.load("case.cfg")
-            holder = cfg.desc(cfg.load_medium(), "fp32")
-        a = Simulation(holder)
-        os.environ["PHP_X2"] = "1"
-        try:
-            b = Simulation(holder)
-        finally:
-            os.environ.pop("PHP_X2", None)
-        a.step(25)
-        b.step(25)
-        for comp in range(9):
-            x, y = a.read_volume(comp), b.read_volume(comp)
-            scale = max(float(np.max(np.abs(x))), 1e-30)
-            assert float(np.max(np.abs(x - y))) <= 1e-5 * scale, (name, comp)
-        a.close()
-        b.close()

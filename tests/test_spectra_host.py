@@ -39,8 +39,12 @@ def test_source_frequency_from_cfg(tmp_path):
             "source type=dipole, x=1,y=1,z=1, wavenumber=1370, component=x\n"
             "source type=gaussian, x=1,y=1,z=1, component=x\n")
     p.write_text(text)
-    v = C.c_double()
-    assert _abi.host_lib().php_spectra_source_frequency(str(p).encode(), C.byref(v)) == 0
+    v, dt = C.c_double(), C.c_double()
+    assert _abi.host_lib().php_spectra_config(str(p).encode(), C.byref(v), C.byref(dt)) == 0
     assert v.value == spectra.source_frequency(text) == 1370 * 0.03e12
+    assert dt.value == -1.0
+    p.write_text(text + "dt = 1.5e-17\n")
+    assert _abi.host_lib().php_spectra_config(str(p).encode(), C.byref(v), C.byref(dt)) == 0
+    assert dt.value == 1.5e-17
     p.write_text("source type=gaussian, x=1\n")
-    assert _abi.host_lib().php_spectra_source_frequency(str(p).encode(), C.byref(v)) != 0
+    assert _abi.host_lib().php_spectra_config(str(p).encode(), C.byref(v), C.byref(dt)) != 0
