@@ -275,33 +275,37 @@ def run_ours(args, ws, rank, local, precision):
     # ---- end to end through the C ABI with host buffers
     e2e = None
     if not args.no_e2e:
-        slice_buf_bytes = 4 * (nx * ny if cfg.output_slice_axis == "z" else (ny * nz if cfg.output_slice_axis == "x" else nx * nz))
-        row_len = 9 + 6 * 0
         sim.sync()
         barrier(ws)
         t0 = time.perf_counter()
         done = 0
         d2h = 0
         h2d = 0
+        pending = []
         while done < args.steps:
             n = min(oi, args.steps - done)
             sim.step(n)                       # per-step source values and DFT phasors copied host -> device
             h2d += n * 8 * (cfg.num_sources + 3)
-            rows = sim.probe_read()           # monitor rows, device -> host
-            d2h += rows.nbytes
-            sim.diagnostics()                 # |E|max, r max, device -> host
-            d2h += 32
-            sim.read_slice("Ez", cfg.output_slice_axis, cfg.output_slice_position)
-            d2h += slice_buf_bytes
+            # the output frame of this interval (monitor rows, |E|max / r max,
+            # the slice) copied device -> host behind the steps; the host
+            # takes it while the device runs the next interval
+            pending.append(sim.frame_begin(diag=True, probe=True,
+                                           slice=("Ez", cfg.output_slice_axis, cfg.output_slice_position)))
+            if len(pending) > 1:
+                fr = sim.frame_wait(pending.pop(0))
+                d2h += fr["rows"].nbytes + 32 + fr["slice"].nbytes
             done += n
+        for tk in pending:
+            fr = sim.frame_wait(tk)
+            d2h += fr["rows"].nbytes + 32 + fr["slice"].nbytes
         sim.sync()
         t1 = time.perf_counter()
         barrier(ws)
         e2e_s = max_over_ranks(t1 - t0, ws)
         e2e = {"value": round(V * args.steps * ws / e2e_s / 1e9, 4), "unit": "Gcell-updates/s",
                "h2d_bytes_per_step": round(h2d / args.steps, 1), "d2h_bytes_per_step": round(d2h / args.steps, 1),
-               "path": "php_step/php_probe_read/php_diagnostics/php_read_slice per output interval "
-                       f"({oi} steps), host buffers"}
+               "path": "php_step + php_frame_begin/php_frame_wait (monitor rows, diagnostics, slice) per output "
+                       f"interval ({oi} steps), page-locked host buffers, one frame in flight"}
 
     s = 4 if precision == "fp32" else 8
     c = census(cfg, medium)

@@ -214,6 +214,53 @@ int php_read_cell_state(php_ctx* ctx, int32_t i, int32_t j, int32_t k, int32_t* 
 /* Global maxima of fdtd.c:3537-3597 for the current state. */
 int php_diagnostics(php_ctx* ctx, php_diag* out);
 
+/* --- asynchronous output frames (fdtd.c:3535-3883 off the device's path) --- */
+
+/* An output frame holds what the writer of one output step reads: the
+ * diagnostics (with the fields and lattice state of the cell of max |r|,
+ * which the divergence report prints, fdtd.c:3626-3663), one slice, the
+ * probe rows recorded since the last frame, and the fields and lattice
+ * state of the full-monitor cell.  php_frame_begin enqueues the gathers and
+ * their copies into page-locked host memory on the context's stream, behind
+ * the steps enqueued so far, and returns at once: the device goes on with
+ * the next php_step while another host thread waits for the frame
+ * (php_frame_wait), writes the files and releases it.  Frames are taken and
+ * released in ticket order; the library holds PHP_FRAME_SLOTS of them, and
+ * php_frame_begin waits (at most 60 s, then PHP_ERR_TIMEOUT) for the oldest
+ * to be released when all are taken.  php_frame_wait and php_frame_release
+ * may run on another thread than the one that steps the context. */
+#define PHP_FRAME_SLOTS 3
+#define PHP_FRAME_MAX_N3 192
+
+typedef struct php_frame_req {
+    int32_t diag;        /* 1: php_diagnostics, and the max |r| cell's state */
+    int32_t slice_comp;  /* php_read_slice component; -1: no slice */
+    int32_t slice_axis;  /* 'x', 'y' or 'z' */
+    int32_t slice_pos;
+    int32_t probe;       /* 1: the probe rows recorded since the last read */
+    int32_t point[3];    /* php_read_point (i, j, k); point[0] < 0: none */
+    int32_t cell[3];     /* php_read_cell_state r, v of (i, j, k); cell[0] < 0: none */
+} php_frame_req;
+
+typedef struct php_frame {
+    int32_t step;                       /* steps done when the frame was taken */
+    int32_t nrows, row_len;             /* probe rows */
+    int32_t diag_natom, cell_natom;
+    int32_t pad_;
+    php_diag diag;
+    double diag_point[9];               /* php_read_point at argmax_r[0..2] */
+    double diag_r[PHP_FRAME_MAX_N3], diag_v[PHP_FRAME_MAX_N3];
+    double point[9];
+    double cell_r[PHP_FRAME_MAX_N3], cell_v[PHP_FRAME_MAX_N3];
+    const float* slice;                 /* slice_len values; valid until release */
+    int64_t slice_len;
+    const double* rows;                 /* nrows x row_len; valid until release */
+} php_frame;
+
+int php_frame_begin(php_ctx* ctx, const php_frame_req* req, int32_t* ticket);
+int php_frame_wait(php_ctx* ctx, int32_t ticket, php_frame* out);
+int php_frame_release(php_ctx* ctx, int32_t ticket);
+
 /* --- per-step probe (monitor_point, fdtd.c:3806-3883) ---------------------- */
 
 /* Records, at the end of every subsequent step, the 9 field values at

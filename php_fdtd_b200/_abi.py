@@ -54,6 +54,21 @@ class Diag(C.Structure):
     _fields_ = [("max_e", _d), ("max_ex", _d), ("max_r", _d), ("argmax_r", _i * 5), ("pad_", _i)]
 
 
+FRAME_MAX_N3 = 192
+
+
+class FrameReq(C.Structure):
+    _fields_ = [("diag", _i), ("slice_comp", _i), ("slice_axis", _i), ("slice_pos", _i), ("probe", _i),
+                ("point", _i * 3), ("cell", _i * 3)]
+
+
+class Frame(C.Structure):
+    _fields_ = [("step", _i), ("nrows", _i), ("row_len", _i), ("diag_natom", _i), ("cell_natom", _i), ("pad_", _i),
+                ("diag", Diag), ("diag_point", _d * 9), ("diag_r", _d * FRAME_MAX_N3), ("diag_v", _d * FRAME_MAX_N3),
+                ("point", _d * 9), ("cell_r", _d * FRAME_MAX_N3), ("cell_v", _d * FRAME_MAX_N3),
+                ("slice", C.POINTER(C.c_float)), ("slice_len", C.c_int64), ("rows", C.POINTER(C.c_double))]
+
+
 class ServerDesc(C.Structure):
     _fields_ = [("abi_version", _i), ("device", _i), ("memory_budget", C.c_uint64), ("max_active", _i),
                 ("chunk_steps", _i)]
@@ -113,6 +128,9 @@ DEVICE_SYMBOLS = {
     "php_diagnostics": (_i, [C.c_void_p, C.POINTER(Diag)]),
     "php_probe_set": (_i, [C.c_void_p, _i, _i, _i, _i]),
     "php_probe_read": (_i, [C.c_void_p, _dp, _i, C.POINTER(_i), C.POINTER(_i)]),
+    "php_frame_begin": (_i, [C.c_void_p, C.POINTER(FrameReq), C.POINTER(_i)]),
+    "php_frame_wait": (_i, [C.c_void_p, _i, C.POINTER(Frame)]),
+    "php_frame_release": (_i, [C.c_void_p, _i]),
     "php_dft_add": (_i, [C.c_void_p, _i, _i, _i, _i, _i, _dp, _i, C.POINTER(_i)]),
     "php_dft_read": (_i, [C.c_void_p, _i, _dp, C.POINTER(_i)]),
     "php_memory_bytes": (_i, [C.c_void_p, C.POINTER(C.c_uint64)]),
@@ -154,7 +172,7 @@ HOST_SYMBOLS = {
 
 _STRUCTS = {"php_desc": Desc, "php_material_desc": MaterialDesc, "php_source_desc": SourceDesc, "php_diag": Diag,
             "php_server_desc": ServerDesc, "php_dft_request": DftRequest, "php_job_info": JobInfo,
-            "php_server_stats": ServerStats,
+            "php_server_stats": ServerStats, "php_frame_req": FrameReq, "php_frame": Frame,
             "php_cfg": Cfg, "php_host_material": HostMaterial}
 
 _host = None

@@ -76,8 +76,9 @@ def build_cli(verbose: bool = False) -> Path:
     out = PKG / "fdtd_b200"
     deps = [HOST / "fdtd_b200_main.c", INC / "php_host.h", INC / "php_fdtd.h", PKG / "libphphost.so", PKG / "libphpfdtd.so"]
     if _stale(out, deps):
-        _run([_cc(), "-O2", "-std=gnu11", f"-I{INC}", HOST / "fdtd_b200_main.c", f"-L{PKG}", "-lphphost", "-lphpfdtd",
-              "-Wl,-rpath,$ORIGIN", "-lm", "-o", out], verbose)
+        _run([_cc(), "-O2", "-std=gnu11", "-pthread", "-Wall", "-Wextra", "-Wno-unused-parameter", f"-I{INC}",
+              HOST / "fdtd_b200_main.c", f"-L{PKG}", "-lphphost", "-lphpfdtd", "-Wl,-rpath,$ORIGIN", "-lm", "-o", out],
+             verbose)
     return out
 
 

@@ -17,6 +17,8 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -25,6 +27,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 using namespace phpdev;
@@ -138,6 +141,30 @@ struct php_ctx {
     IonMaps ion_maps;
     int n3_ion = 0;
     int ion_off_ref = 0;
+    /* the few-atom material (N <= 4) with the most cells: its coefficients
+     * ride in the sweep's kernel parameters (StepArgs::ion_k) */
+    int ion_k_off = -1;
+    std::vector<double> ion_k;
+    std::vector<double> iso_scale;   /* StepArgs::iso, per material */
+
+    /* output frames (php_frame_begin): page-locked slots taken in ticket
+     * order; state 0 free, 1 taken (begun and not released) */
+    struct FrameSlot {
+        std::atomic<int> state{0};
+        int32_t ticket = -1, step = 0;
+        php_frame_req req{};
+        int64_t rows_copied = 0, slice_len = 0;
+        int32_t row_len = 0;
+        cudaEvent_t done = nullptr;
+        FrameHead* head = nullptr;   /* pinned */
+        float* slice = nullptr;      /* pinned */
+        double* rows = nullptr;      /* pinned */
+        size_t rows_bytes = 0;
+    };
+    FrameSlot frames[PHP_FRAME_SLOTS];
+    int32_t frame_next = 0;
+    FrameHead* frame_head_dev = nullptr;
+    int32_t probe_t0 = 0;        /* step of the last probe read (rows pending = t - probe_t0) */
 };
 
 /* ------------------------------------------------------------------ utils */
@@ -483,6 +510,9 @@ static StepArgs<R> make_args(php_ctx* ctx, int s_local)
     a.r = (R*)ctx->r;
     a.v = (R*)ctx->v;
     a.pr = ctx->ion_split ? (const R*)ctx->Pr : nullptr;
+    a.ion_k_off = ctx->ion_k_off;
+    for (size_t q = 0; q < ctx->ion_k.size() && q < (size_t)kIonK; q++) a.ion_k[q] = (R)ctx->ion_k[q];
+    for (size_t q = 0; q < ctx->iso_scale.size() && q < (size_t)kIsoMats; q++) a.iso[q] = (R)ctx->iso_scale[q];
     a.nslot = ctx->nslot;
 #ifndef PHP_SMEM_MATS
 #define PHP_SMEM_MATS 0
@@ -721,7 +751,11 @@ static int upload_tables(php_ctx* ctx, const std::vector<MatD>& mats, const std:
                          const std::vector<double>& ion_coef, const AxisD* axes)
 {
     std::vector<MatCoef<R>> mc(mats.size());
-    for (size_t i = 0; i < mats.size(); i++) mc[i] = pack_material<R>(ctx, mats[i], ion_off[i]);
+    ctx->iso_scale.assign(mats.size(), 0.0);
+    for (size_t i = 0; i < mats.size(); i++) {
+        mc[i] = pack_material<R>(ctx, mats[i], ion_off[i]);
+        if (mc[i].flags & kIso) ctx->iso_scale[i] = (double)mc[i].eps_inv[0];
+    }
     int rc = dalloc(ctx, &ctx->mc, mc.size() * sizeof(MatCoef<R>));
     if (rc) return rc;
     CK(cudaMemcpyAsync(ctx->mc, mc.data(), mc.size() * sizeof(MatCoef<R>), cudaMemcpyHostToDevice, ctx->stream));
@@ -799,6 +833,12 @@ static void ctx_free(php_ctx* ctx)
     for (int b = 0; b < 2; ++b) {
         pinned_put(ctx->step_in_host[b]);
         if (ctx->staged[b]) cudaEventDestroy(ctx->staged[b]);
+    }
+    for (auto& f : ctx->frames) {
+        if (f.done) cudaEventDestroy(f.done);
+        pinned_put(f.head);
+        pinned_put(f.slice);
+        pinned_put(f.rows);
     }
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -976,6 +1016,7 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
     std::vector<int64_t> slot_cell;
     std::vector<int32_t> slot_n3;
     int n3max = 0;
+    std::vector<int64_t> mat_cells(d.num_materials, 0);
     for (int k = 0; k < nz; k++)
         for (int j = 0; j < ny; j++)
             for (int i = 0; i < nx; i++) {
@@ -985,6 +1026,7 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
                                 k, d.num_materials - 1);
                 const int64_t c = ((int64_t)k * ny + j) * nxp + i;
                 mat_dev[c] = (uint8_t)id;
+                mat_cells[id]++;
                 if (mats[id].flags & (kAde | kAtoms)) {
                     slot_cell.push_back(c);
                     slot_n3.push_back(3 * mats[id].natom);
@@ -1002,6 +1044,24 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
     }
     ctx->nslot = (int64_t)slot_cell.size();
     ctx->n3max = n3max;
+    {
+        int best = -1;
+        for (int i = 0; i < d.num_materials; i++)
+            if ((mats[i].flags & kAtoms) && mats[i].natom <= 4 && mat_cells[i] > 0 && (best < 0 || mat_cells[i] > mat_cells[best]))
+                best = i;
+        if (best >= 0) {
+            const int N = mats[best].natom, n3 = 3 * N;
+            const php_material_desc& M = d.materials[best];
+            ctx->ion_k.assign(kIonK, 0.0);
+            for (int q = 0; q < 9 * N; q++) {
+                ctx->ion_k[q] = M.qezv[q];
+                ctx->ion_k[kIonKM + q] = M.qezm[q];
+            }
+            for (int q = 0; q < n3; q++)
+                for (int p = 0; p < n3; p++) ctx->ion_k[kIonKD + q * kIonKQ + p] = M.dmm[(size_t)q * n3 + p];
+            ctx->ion_k_off = ion_off[best];
+        }
+    }
     const int namax = n3max / 3;
     ctx->namax_tpl = namax == 0 ? 0 : namax <= 2 ? 2 : namax <= 4 ? 4 : namax <= 8 ? 8 : namax <= 16 ? 16 : 64;
     if (namax > 64) return fail(ctx, PHP_ERR_UNSUPPORTED, "natom %d above the supported 64", namax);
@@ -1277,6 +1337,25 @@ static int stage_step_inputs(php_ctx* ctx, int n, int b)
 
 /* ------------------------------------------------------------- public API */
 
+/* frame gathers (php_frame_begin) */
+
+static int64_t point_index(const php_ctx* ctx, const int32_t* p)
+{
+    return ((int64_t)p[2] * ctx->ny + p[1]) * ctx->nxp + p[0];
+}
+
+template <typename R>
+static void launch_frame_gather(php_ctx* ctx, const DiagPartial* fin, int has_point, int64_t pc, int64_t cc)
+{
+    R* const* fp = reinterpret_cast<R* const*>(ctx->f);
+    Fields<R> f{fp[0], fp[1], fp[2], fp[3], fp[4], fp[5], fp[6], fp[7], fp[8]};
+    frame_gather<R><<<1, 256, 0, ctx->stream>>>(f, ctx->mat, ctx->slot, (const MatCoef<R>*)ctx->mc, (const R*)ctx->r,
+                                                 (const R*)ctx->v, ctx->nslot, ctx->nx, ctx->ny, ctx->nz, ctx->nxp,
+                                                 ctx->n3max, fin, has_point, pc, cc,
+                                                 ctx->probe ? ctx->probe_count : nullptr, ctx->err_flag,
+                                                 ctx->frame_head_dev);
+}
+
 extern "C" {
 
 int php_create(const php_desc* desc, php_ctx** out)
@@ -1447,12 +1526,10 @@ int php_get_step(const php_ctx* ctx, int32_t* t)
     return PHP_OK;
 }
 
-static int read_slice_impl(php_ctx* ctx, int32_t comp, char axis, int32_t position, void* out, bool f32)
+/* Gather geometry of a slice, with the reference's messages for bad ones. */
+static int slice_geom(php_ctx* ctx, int32_t comp, char axis, int32_t position, int& ax, int& pos, size_t& n)
 {
-    if (!ctx || !out) return PHP_ERR_INPUT;
     if (comp < 0 || comp > 9) return fail(ctx, PHP_ERR_INPUT, "bad component %d", comp);
-    int ax, pos;
-    size_t n;
     if (axis == 'z') {
         if (position < 0 || position >= ctx->nz) return fail(ctx, PHP_ERR_INPUT, "Error: No process contains slice z=%d", position);
         ax = 0;
@@ -1473,6 +1550,16 @@ static int read_slice_impl(php_ctx* ctx, int32_t comp, char axis, int32_t positi
     } else {
         return fail(ctx, PHP_ERR_INPUT, "Error: Invalid slice axis '%c'. Must be 'x', 'y', or 'z'.", axis);
     }
+    return PHP_OK;
+}
+
+static int read_slice_impl(php_ctx* ctx, int32_t comp, char axis, int32_t position, void* out, bool f32)
+{
+    if (!ctx || !out) return PHP_ERR_INPUT;
+    int ax, pos;
+    size_t n;
+    int rc = slice_geom(ctx, comp, axis, position, ax, pos, n);
+    if (rc) return rc;
     if (ctx->prec == PHP_PREC_FP32) launch_gather_plane<float>(ctx, comp, ax, pos, f32);
     else launch_gather_plane<double>(ctx, comp, ax, pos, f32);
     CK(cudaGetLastError());
@@ -1599,12 +1686,13 @@ int php_read_cell_state(php_ctx* ctx, int32_t i, int32_t j, int32_t k, int32_t* 
     return PHP_OK;
 }
 
-int php_diagnostics(php_ctx* ctx, php_diag* out)
+/* Enqueues the two diagnostics passes; the result lands in *fin (scratch). */
+static int enqueue_diag(php_ctx* ctx, DiagPartial** fin_out)
 {
-    if (!ctx || !out) return PHP_ERR_INPUT;
     const int blocks = 148 * 4;
     DiagPartial* part = (DiagPartial*)ctx->scratch;
     DiagPartial* fin = part + blocks;
+    *fin_out = fin;
     if (ctx->prec == PHP_PREC_FP32) {
         float* const* fp = reinterpret_cast<float* const*>(ctx->f);
         Fields<float> f{fp[0], fp[1], fp[2], fp[3], fp[4], fp[5], fp[6], fp[7], fp[8]};
@@ -1620,10 +1708,12 @@ int php_diagnostics(php_ctx* ctx, php_diag* out)
     }
     diag_pass2<<<1, 256, 0, ctx->stream>>>(part, blocks, fin);
     CK(cudaGetLastError());
-    DiagPartial h;
-    CK(cudaMemcpyAsync(ctx->host_stage, fin, sizeof(DiagPartial), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    memcpy(&h, ctx->host_stage, sizeof(h));
+    return PHP_OK;
+}
+
+/* php_diag from the reduced partial (argmax in the reference's loop order) */
+static void decode_diag(const php_ctx* ctx, const DiagPartial& h, php_diag* out)
+{
     out->max_e = h.max_e;
     out->max_ex = h.max_ex;
     out->max_r = h.max_r;
@@ -1640,6 +1730,19 @@ int php_diagnostics(php_ctx* ctx, php_diag* out)
     } else {
         for (int q = 0; q < 5; q++) out->argmax_r[q] = -1;
     }
+}
+
+int php_diagnostics(php_ctx* ctx, php_diag* out)
+{
+    if (!ctx || !out) return PHP_ERR_INPUT;
+    DiagPartial* fin = nullptr;
+    int rc = enqueue_diag(ctx, &fin);
+    if (rc) return rc;
+    DiagPartial h;
+    CK(cudaMemcpyAsync(ctx->host_stage, fin, sizeof(DiagPartial), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    memcpy(&h, ctx->host_stage, sizeof(h));
+    decode_diag(ctx, h, out);
     return PHP_OK;
 }
 
@@ -1666,6 +1769,7 @@ int php_probe_set(php_ctx* ctx, int32_t i, int32_t j, int32_t k_field, int32_t k
     }
     CK(cudaMemsetAsync(ctx->probe_count, 0, 2 * sizeof(int32_t), ctx->stream));
     ctx->probe = true;
+    ctx->probe_t0 = ctx->t;
     return PHP_OK;
 }
 
@@ -1685,6 +1789,140 @@ int php_probe_read(php_ctx* ctx, double* rows, int32_t max_rows, int32_t* nrows,
     CK(cudaMemsetAsync(ctx->probe_count, 0, 2 * sizeof(int32_t), ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     *nrows = cnt[0];
+    ctx->probe_t0 = ctx->t;
+    return PHP_OK;
+}
+
+/* ------------------------------------------------------------ output frames */
+
+int php_frame_begin(php_ctx* ctx, const php_frame_req* req, int32_t* ticket)
+{
+    if (!ctx || !req || !ticket) return PHP_ERR_INPUT;
+    int ax = 0, pos = 0;
+    size_t slice_n = 0;
+    if (req->slice_comp >= 0) {
+        int rc = slice_geom(ctx, req->slice_comp, (char)req->slice_axis, req->slice_pos, ax, pos, slice_n);
+        if (rc) return rc;
+    }
+    const bool has_point = req->point[0] >= 0;
+    if (has_point && (req->point[0] >= ctx->nx || req->point[1] < 0 || req->point[1] >= ctx->ny || req->point[2] < -1 ||
+                      req->point[2] > ctx->nz))
+        return fail(ctx, PHP_ERR_INPUT, "point (%d,%d,%d) outside the grid", req->point[0], req->point[1], req->point[2]);
+    const bool has_cell = req->cell[0] >= 0;
+    if (has_cell && (req->cell[0] >= ctx->nx || req->cell[1] < 0 || req->cell[1] >= ctx->ny || req->cell[2] < 0 ||
+                     req->cell[2] >= ctx->nz))
+        return fail(ctx, PHP_ERR_INPUT, "cell (%d,%d,%d) outside the grid", req->cell[0], req->cell[1], req->cell[2]);
+    if (req->probe && !ctx->probe) return fail(ctx, PHP_ERR_STATE, "no probe set");
+    if (!ctx->frame_head_dev) {
+        int rc = dalloc(ctx, (void**)&ctx->frame_head_dev, sizeof(FrameHead));
+        if (rc) return rc;
+    }
+    const int32_t tk = ctx->frame_next;
+    php_ctx::FrameSlot& F = ctx->frames[tk % PHP_FRAME_SLOTS];
+    /* the oldest frame must have been released (bounded wait) */
+    const auto t0 = std::chrono::steady_clock::now();
+    while (F.state.load(std::memory_order_acquire) != 0) {
+        if (std::chrono::steady_clock::now() - t0 > std::chrono::seconds(60))
+            return fail(ctx, PHP_ERR_TIMEOUT, "frame %d was not released within 60 s", F.ticket);
+        std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+    if (!F.done) CK(cudaEventCreateWithFlags(&F.done, cudaEventDisableTiming));
+    if (!F.head) F.head = (FrameHead*)pinned_get(sizeof(FrameHead));
+    const size_t slice_cap = std::max({(size_t)ctx->nx * ctx->ny, (size_t)ctx->ny * ctx->nz, (size_t)ctx->nx * ctx->nz});
+    if (!F.slice) F.slice = (float*)pinned_get(slice_cap * sizeof(float));
+    const int32_t row_len = 9 + 2 * ctx->probe_n3;
+    int64_t rows = 0;
+    if (req->probe) {
+        rows = std::min<int64_t>((int64_t)ctx->t - ctx->probe_t0, kProbeCap);
+        const size_t need = (size_t)std::max<int64_t>(rows, 1) * row_len * sizeof(double);
+        if (F.rows_bytes < need) {
+            pinned_put(F.rows);
+            F.rows = (double*)pinned_get(need);
+            F.rows_bytes = F.rows ? need : 0;
+        }
+        if (!F.rows) return fail(ctx, PHP_ERR_OOM, "page-locked host allocation failed");
+    }
+    if (!F.head || !F.slice) return fail(ctx, PHP_ERR_OOM, "page-locked host allocation failed");
+
+    DiagPartial* fin = nullptr;
+    if (req->diag) {
+        int rc = enqueue_diag(ctx, &fin);
+        if (rc) return rc;
+    }
+    const int64_t pc = has_point ? point_index(ctx, req->point) : 0;
+    const int64_t cc = has_cell ? point_index(ctx, req->cell) : -1;
+    if (ctx->prec == PHP_PREC_FP32) launch_frame_gather<float>(ctx, fin, has_point, pc, cc);
+    else launch_frame_gather<double>(ctx, fin, has_point, pc, cc);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(F.head, ctx->frame_head_dev, sizeof(FrameHead), cudaMemcpyDeviceToHost, ctx->stream));
+    if (req->slice_comp >= 0) {
+        if (ctx->prec == PHP_PREC_FP32) launch_gather_plane<float>(ctx, req->slice_comp, ax, pos, true);
+        else launch_gather_plane<double>(ctx, req->slice_comp, ax, pos, true);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(F.slice, ctx->scratch, slice_n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    if (req->probe) {
+        if (rows > 0)
+            CK(cudaMemcpyAsync(F.rows, ctx->probe_rows, (size_t)rows * row_len * sizeof(double), cudaMemcpyDeviceToHost,
+                               ctx->stream));
+        CK(cudaMemsetAsync(ctx->probe_count, 0, 2 * sizeof(int32_t), ctx->stream));
+        ctx->probe_t0 = ctx->t;
+    }
+    CK(cudaEventRecord(F.done, ctx->stream));
+    F.ticket = tk;
+    F.step = ctx->t;
+    F.req = *req;
+    F.rows_copied = rows;
+    F.row_len = row_len;
+    F.slice_len = req->slice_comp >= 0 ? (int64_t)slice_n : 0;
+    F.state.store(1, std::memory_order_release);
+    ctx->frame_next++;
+    *ticket = tk;
+    return PHP_OK;
+}
+
+int php_frame_wait(php_ctx* ctx, int32_t ticket, php_frame* out)
+{
+    if (!ctx || !out || ticket < 0) return PHP_ERR_INPUT;
+    php_ctx::FrameSlot& F = ctx->frames[ticket % PHP_FRAME_SLOTS];
+    if (F.state.load(std::memory_order_acquire) != 1 || F.ticket != ticket)
+        return fail(ctx, PHP_ERR_STATE, "frame %d is not taken", ticket);
+    CK(cudaEventSynchronize(F.done));
+    const FrameHead& h = *F.head;
+    if (h.err) return fail(ctx, PHP_ERR_TIMEOUT, "a sweep kernel gave up waiting for its plane loads");
+    memset(out, 0, sizeof(*out));
+    out->step = F.step;
+    if (F.req.diag) {
+        decode_diag(ctx, h.diag, &out->diag);
+        out->diag_natom = h.diag_natom;
+        memcpy(out->diag_point, h.diag_point, sizeof(out->diag_point));
+        memcpy(out->diag_r, h.diag_r, sizeof(out->diag_r));
+        memcpy(out->diag_v, h.diag_v, sizeof(out->diag_v));
+    }
+    if (F.req.point[0] >= 0) memcpy(out->point, h.point, sizeof(out->point));
+    if (F.req.cell[0] >= 0) {
+        out->cell_natom = h.cell_natom;
+        memcpy(out->cell_r, h.cell_r, sizeof(out->cell_r));
+        memcpy(out->cell_v, h.cell_v, sizeof(out->cell_v));
+    }
+    out->slice = F.slice_len ? F.slice : nullptr;
+    out->slice_len = F.slice_len;
+    out->row_len = F.row_len;
+    if (F.req.probe) {
+        if (h.probe_count[1])
+            return fail(ctx, PHP_ERR_STATE, "probe buffer overflowed (more than %d rows between reads)", kProbeCap);
+        out->nrows = (int32_t)std::min<int64_t>(h.probe_count[0], F.rows_copied);
+        out->rows = F.rows;
+    }
+    return PHP_OK;
+}
+
+int php_frame_release(php_ctx* ctx, int32_t ticket)
+{
+    if (!ctx || ticket < 0) return PHP_ERR_INPUT;
+    php_ctx::FrameSlot& F = ctx->frames[ticket % PHP_FRAME_SLOTS];
+    if (F.ticket != ticket) return fail(ctx, PHP_ERR_STATE, "frame %d is not taken", ticket);
+    F.state.store(0, std::memory_order_release);
     return PHP_OK;
 }
 

@@ -190,7 +190,11 @@ struct IonPipe {
     /* per stage: r, v, then the slots' cell offsets (int64, 1024 B), atom
      * coordinate counts (int32, 512 B) and material ids (uint8, 128 B) */
     static constexpr uint32_t IDX = 2048;
-    static constexpr uint32_t STAGE = 2 * BOX + IDX;
+    /* then the crystal-frame inputs: Ex, Ey, Ez of the tile's cells, gathered
+     * by the producer warp with cp.async */
+    static constexpr uint32_t E_OFF = 2 * BOX + IDX;
+    static constexpr uint32_t EB = 3 * kIonTile * sizeof(R);
+    static constexpr uint32_t STAGE = 2 * BOX + IDX + EB;
     static constexpr uint32_t A_BYTES = kIonTile * NP * 2;           /* bf16 rows of one group */
     static constexpr uint32_t B_BYTES = NP * NP * 2;
     static constexpr uint32_t OPS = TC ? GROUPS * 2 * A_BYTES + 2 * B_BYTES : NP * NP * sizeof(R);
@@ -239,12 +243,27 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar)
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
+/* B-byte asynchronous copy global -> shared (B = 4, 8 or 16) */
+template <int B>
+__device__ __forceinline__ void cp_async_ca(void* dst, const void* src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_addr(dst)), "l"(src), "n"(B) : "memory");
+}
+
+/* an arrival on bar once this thread's earlier cp.async copies have landed
+ * (counted in the barrier's expected arrivals) */
+__device__ __forceinline__ void cp_async_arrive_noinc(uint64_t* bar)
+{
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
 template <typename R, int NP, int S>
 __global__ void __launch_bounds__(IonPipe<R, NP, S>::THREADS, 1)
     ion_pipe(const __grid_constant__ IonArgs<R> a, const __grid_constant__ IonMaps maps, int32_t n3)
 {
     using P = IonPipe<R, NP, S>;
     static_assert(NP % 16 == 0 && NP >= 16 && NP <= 64, "3N padded to 16..64");
+    static_assert(P::SMEM <= 227u * 1024u, "shared memory of one CTA");
     extern __shared__ __align__(128) unsigned char dyn_smem[];
     unsigned char* base = dyn_smem + ((1024u - (smem_addr(dyn_smem) & 1023u)) & 1023u);
     unsigned char* stages = base;
@@ -278,7 +297,8 @@ __global__ void __launch_bounds__(IonPipe<R, NP, S>::THREADS, 1)
     }
     if (tid == 0) {
         for (int q = 0; q < S; ++q) {
-            mbar_init(&full[q], 1);
+            /* the producer's expect_tx arrival and one cp.async arrival per producer lane */
+            mbar_init(&full[q], 1 + 32);
             mbar_init(&empty[q], 1);
         }
         for (int g = 0; g < P::GROUPS; ++g) mbar_init(&mma_bar[g], 1);
@@ -295,16 +315,19 @@ __global__ void __launch_bounds__(IonPipe<R, NP, S>::THREADS, 1)
 
     if (warp == P::GROUPS * 4) {
         /* ------------------------------------------------------ producer */
-        if ((tid & 31) == 0) {
-            int issued = 0;
-            for (int k = 0; k < mine; ++k) {
-                const int st = k % S;
-                if (k >= S && !mbar_wait(&empty[st], ((k / S) - 1) & 1)) {
-                    failed = true;
-                    break;
-                }
-                const int x = ((int)blockIdx.x + k * (int)gridDim.x) * kIonTile;
-                unsigned char* b = stages + st * P::STAGE;
+        const int lane = tid & 31;
+        int issued = 0;
+        for (int k = 0; k < mine; ++k) {
+            const int st = k % S;
+            bool ok = true;
+            if (k >= S && lane == 0) ok = mbar_wait(&empty[st], ((k / S) - 1) & 1);
+            if (!__shfl_sync(0xffffffffu, ok ? 1 : 0, 0)) {
+                failed = true;
+                break;
+            }
+            const int x = ((int)blockIdx.x + k * (int)gridDim.x) * kIonTile;
+            unsigned char* b = stages + st * P::STAGE;
+            if (lane == 0) {
                 /* slots left in this tile: a multiple of 32 (the pool is padded) */
                 const uint32_t nrem = (uint32_t)min((int64_t)kIonTile, a.nslot - x);
                 mbar_arrive_expect_tx(&full[st], tx_bytes + nrem * 13u);
@@ -313,13 +336,28 @@ __global__ void __launch_bounds__(IonPipe<R, NP, S>::THREADS, 1)
                 bulk_load(b + 2 * P::BOX, a.slot_cell + x, nrem * 8u, &full[st]);
                 bulk_load(b + 2 * P::BOX + 1024, a.slot_n3 + x, nrem * 4u, &full[st]);
                 bulk_load(b + 2 * P::BOX + 1536, a.slot_mat + x, nrem, &full[st]);
-                issued = k + 1;
             }
-            if (failed) {
-                atomicExch(a.err, 1);
-                /* loads issued and not consumed land before the CTA leaves */
-                for (int k = *consumed; k < issued; ++k) mbar_wait(&full[k % S], (k / S) & 1);
+            /* E^{n+1} of the tile's cells, gathered ahead like the rest of the
+             * stage (padding slots repeat the last cell; slots past the pool
+             * are not read) */
+            R* es = reinterpret_cast<R*>(b + P::E_OFF);
+#pragma unroll
+            for (int u = 0; u < kIonTile / 32; ++u) {
+                const int t = lane + 32 * u;
+                if ((int64_t)x + t < a.nslot) {
+                    const int64_t c = a.slot_cell[x + t];
+                    cp_async_ca<sizeof(R)>(es + t, a.ex + c);
+                    cp_async_ca<sizeof(R)>(es + kIonTile + t, a.ey + c);
+                    cp_async_ca<sizeof(R)>(es + 2 * kIonTile + t, a.ez + c);
+                }
             }
+            cp_async_arrive_noinc(&full[st]);
+            issued = k + 1;
+        }
+        if (failed && lane == 0) {
+            atomicExch(a.err, 1);
+            /* loads issued and not consumed land before the CTA leaves */
+            for (int k = *consumed; k < issued; ++k) mbar_wait(&full[k % S], (k / S) & 1);
         }
     } else {
         /* ------------------------------------------------------ consumers */
@@ -348,11 +386,11 @@ __global__ void __launch_bounds__(IonPipe<R, NP, S>::THREADS, 1)
             R e0 = R(0), e1 = R(0), e2 = R(0);
             const MatCoef<R>* mp = nullptr;
             if (n3c) {
-                const int64_t c = reinterpret_cast<const int64_t*>(sb + 2 * P::BOX)[gt];
+                const R* es = reinterpret_cast<const R*>(sb + P::E_OFF);
                 mp = &a.mc[(sb + 2 * P::BOX + 1536)[gt]];
-                e0 = a.ex[c];
-                e1 = a.ey[c];
-                e2 = a.ez[c];
+                e0 = es[gt];
+                e1 = es[kIonTile + gt];
+                e2 = es[2 * kIonTile + gt];
                 rot_fwd<false>(mp->flags, mp->cs, mp->sn, e0, e1, e2);
             }
             R p0 = R(0), p1 = R(0), p2 = R(0);

@@ -90,6 +90,15 @@ struct Psi {
     R *dxy, *dxz, *dyx, *dyz, *dzx, *dzy;
 };
 
+/* The fused sweep's copy of one few-atom material's ion coefficients in the
+ * kernel parameters (constant bank): QeZV [9 N], QeZM [9 N] and DMM with row
+ * stride kIonKQ, for N <= 4 */
+constexpr int kIonKQ = 12;
+constexpr int kIonKM = 36;
+constexpr int kIonKD = 72;
+constexpr int kIonK = kIonKD + kIonKQ * kIonKQ;
+constexpr int kIsoMats = 32;
+
 template <typename R>
 struct StepArgs {
     Fields<R> f;
@@ -101,6 +110,12 @@ struct StepArgs {
     const R* ion_coef;
     R *P, *Po, *r, *v;         /* pools */
     const R* pr;               /* QeZV . r [3][nslot] when the ion pass runs apart (php_ions.cuh), else null */
+    int32_t ion_k_off;         /* ion_coef offset of the material copied in ion_k, -1 for none */
+    R ion_k[kIonK];
+    /* E = iso[id] * D for the plain isotropic materials (kIso) among the
+     * first kIsoMats ids, 0 for the others: the fused sweep's common case
+     * without a load of the material record */
+    R iso[kIsoMats];
     int64_t nslot;
     int32_t nmat;
     int32_t nx, ny, nz, nxp, L, zchunk;
@@ -329,6 +344,91 @@ __global__ void __launch_bounds__(256) diag_pass2(const DiagPartial* scratch, in
         __syncthreads();
     }
     if (threadIdx.x == 0) *out = sh[0];
+}
+
+/* ---------------------------------------------------------- output frames */
+
+constexpr int kFrameMaxN3 = 192; /* 3 N for N <= 64 atoms */
+
+/* The small part of an output frame (php_frame_begin), gathered on the
+ * device and copied to page-locked host memory in one piece. */
+struct FrameHead {
+    DiagPartial diag;                                       /* diag_pass2 result */
+    double diag_point[9];                                   /* fields at the max |r| cell */
+    double diag_r[kFrameMaxN3], diag_v[kFrameMaxN3];        /* r, v there */
+    double point[9];                                        /* fields at the requested point */
+    double cell_r[kFrameMaxN3], cell_v[kFrameMaxN3];        /* r, v of the requested cell */
+    int32_t diag_natom, cell_natom;
+    int32_t probe_count[2];                                 /* rows recorded, overflow flag */
+    int32_t err;                                            /* a sweep's bounded wait gave up */
+    int32_t pad_;
+};
+
+/* Field values (Ex Ey Ez Dx Dy Dz Hx Hy Hz) at device cell c, and r, v of the
+ * atom cell c (none when its material has no atoms). */
+template <typename R>
+__device__ __forceinline__ void frame_cell(const Fields<R>& f, const uint8_t* mat, const int32_t* slot,
+                                           const MatCoef<R>* mc, const R* r, const R* v, int64_t nslot,
+                                           int64_t cf, int64_t ca, double* point9, double* rr, double* vv,
+                                           int32_t* natom)
+{
+    const int t = threadIdx.x;
+    if (point9 && t < 9) {
+        const R* p[9] = {f.ex, f.ey, f.ez, f.dx, f.dy, f.dz, f.hx, f.hy, f.hz};
+        point9[t] = (double)p[t][cf];
+    }
+    if (ca < 0) return;
+    const int na = mc[mat[ca]].natom;
+    const int64_t s = (na > 0 && slot) ? slot[ca] : -1;
+    if (t == 0) *natom = s >= 0 ? na : 0;
+    if (s < 0) return;
+    for (int q = t; q < 3 * na && q < kFrameMaxN3; q += blockDim.x) {
+        rr[q] = (double)r[(int64_t)q * nslot + s];
+        vv[q] = (double)v[(int64_t)q * nslot + s];
+    }
+}
+
+/* One block.  fin: the diagnostics of this frame (nullptr: none); the
+ * point's device index (k may be -1 or nz, the halo planes; has_point 0:
+ * none) and the cell's (-1: none); probe_count: the probe row counter
+ * (nullptr: no probe).  Thread 0 writes every natom field. */
+template <typename R>
+__global__ void frame_gather(const Fields<R> f, const uint8_t* mat, const int32_t* slot, const MatCoef<R>* mc,
+                             const R* r, const R* v, int64_t nslot, int nx, int ny, int nz, int nxp, int n3max,
+                             const DiagPartial* fin, int has_point, int64_t point_c, int64_t cell_c,
+                             const int32_t* probe_count,
+                             const int32_t* err, FrameHead* head)
+{
+    const int t = threadIdx.x;
+    if (fin) {
+        const DiagPartial d = *fin;
+        if (t == 0) {
+            head->diag = d;
+            head->diag_natom = 0;
+        }
+        if (d.max_r > 0.0 && d.key_r != INT64_MAX) {
+            /* reference loop order (i, j, k, coordinate), as php_diagnostics decodes it */
+            const int64_t n3 = n3max > 1 ? n3max : 1;
+            int64_t cell = d.key_r / n3;
+            const int k = (int)(cell % nz);
+            cell /= nz;
+            const int j = (int)(cell % ny);
+            const int i = (int)(cell / ny);
+            const int64_t c = ((int64_t)k * ny + j) * nxp + i;
+            frame_cell(f, mat, slot, mc, r, v, nslot, c, c, head->diag_point, head->diag_r, head->diag_v, &head->diag_natom);
+        }
+    }
+    if (has_point)
+        frame_cell<R>(f, mat, slot, mc, r, v, nslot, point_c, -1, head->point, nullptr, nullptr, nullptr);
+    if (cell_c >= 0) {
+        if (t == 0) head->cell_natom = 0;
+        frame_cell<R>(f, mat, slot, mc, r, v, nslot, cell_c, cell_c, nullptr, head->cell_r, head->cell_v, &head->cell_natom);
+    }
+    if (t == 0) {
+        head->probe_count[0] = probe_count ? probe_count[0] : 0;
+        head->probe_count[1] = probe_count ? probe_count[1] : 0;
+        head->err = *err;
+    }
 }
 
 } // namespace phpdev

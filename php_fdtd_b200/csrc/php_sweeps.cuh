@@ -260,6 +260,7 @@ template <typename R>
 struct CellPsi {
     int sz;
     R xy, xz, yx, yz, zx, zy;
+    R kdz;                     /* dt / (dz kappa_z), FP32/FP64 fast paths */
 };
 
 /* psi_D of fdtd.c:3258-3334 (the reads) */
@@ -268,6 +269,9 @@ __device__ __forceinline__ void load_psi_d(const StepArgs<R>& a, int i, int j, i
 {
     const int L2 = 2 * a.L;
     ps.sz = ldg_nh(a.tz.slot + k);
+    /* FP64: the z profile with the other early loads (measured faster);
+     * FP32 reads it in d_update (measured faster there) */
+    ps.kdz = sizeof(R) == 8 ? ldg_nh(a.tz.kd + k) : R(0);
     ps.xy = ps.xz = ps.yx = ps.yz = ps.zx = ps.zy = R(0);
     if (sx >= 0) {
         const int q = (k * a.ny + j) * L2 + sx;
@@ -335,7 +339,8 @@ __device__ __forceinline__ void d_update(const StepArgs<R>& a, int i, int j, int
     } else {
         const R dHzy = hz0 - hz_jm, dHyz = hy0 - hyk, dHxz = hx0 - hxk;
         const R dHzx = hz0 - hz_im, dHyx = hy0 - hy_im, dHxy = hx0 - hx_jm;
-        const R kdx = ldg(a.tx.kd + i), kdy = ldg(a.ty.kd + j), kdz = ldg_nh(a.tz.kd + k);
+        const R kdx = ldg(a.tx.kd + i), kdy = ldg(a.ty.kd + j);
+        const R kdz = sizeof(R) == 8 ? ps.kdz : ldg_nh(a.tz.kd + k);
         /* psi terms enter as zeros outside the PML */
         R ux = kdy * dHzy - kdz * dHyz + ps.yx + ps.zx;
         R uy = -kdx * dHzx + kdz * dHxz + ps.xy + ps.zy;
@@ -364,6 +369,12 @@ __device__ __forceinline__ void d_update(const StepArgs<R>& a, int i, int j, int
     }
 }
 
+/* FP32: E = iso * D from the kernel parameters for plain isotropic cells
+ * (measured 2 % faster on the 256^3 tip workload; FP64 measured slower) */
+#ifndef PHP_ISO_PARAM
+#define PHP_ISO_PARAM 1
+#endif
+
 /* bytes of r (and again of v) per cell up to which the fused sweep holds a
  * cell's ion state in registers: 6 FP32 coordinates (two atoms) fit the
  * 64-register budget of the FP32 sweep without spills, FP64 ones do not */
@@ -383,6 +394,25 @@ __device__ __forceinline__ void for_atoms(int n3, F&& f)
         for (int q = 0; q < n3; ++q) f(q);
     }
 }
+
+/* Coefficient sources of the fused ion update: the material's arrays in
+ * global memory, or the copy in the kernel parameters, which the unrolled
+ * few-atom loops read as constant-bank operands instead of loads. */
+template <typename R>
+struct IonCoefGlobal {
+    const R* qv;
+    int n3;
+    __device__ __forceinline__ R zv(int i) const { return ldg(qv + i); }
+    __device__ __forceinline__ R zm(int i) const { return ldg(qv + 3 * n3 + i); }
+    __device__ __forceinline__ R dmm(int q, int p) const { return ldg(qv + 6 * n3 + q * n3 + p); }
+};
+template <typename R>
+struct IonCoefParam {
+    const StepArgs<R>& a;
+    __device__ __forceinline__ R zv(int i) const { return a.ion_k[i]; }
+    __device__ __forceinline__ R zm(int i) const { return a.ion_k[kIonKM + i]; }
+    __device__ __forceinline__ R dmm(int q, int p) const { return a.ion_k[kIonKD + q * kIonKQ + p]; }
+};
 
 /* D -> E, ADE and ions for one cell (fdtd.c:3404-3528).  ex..ez hold E^n on
  * entry (lab frame) and E^{n+1} on return; dx..dz are D^{n+1}; ix..iz are
@@ -409,46 +439,50 @@ __device__ __forceinline__ void e_update(const StepArgs<R>& a, const MatCoef<R>&
      * few atoms (VREG) r and v of the cell sit in registers and all 2 x 3N
      * loads are issued together here. */
     constexpr int QN = NAMAX > 0 ? 3 * NAMAX : 1;
-    constexpr bool VREG = QN * (int)sizeof(R) <= kIonRegBytes;
+    constexpr bool VREG = NAMAX > 0 && QN * (int)sizeof(R) <= kIonRegBytes;
     R pr0 = R(0), pr1 = R(0), pr2 = R(0);
     R rold[QN];
     R vold[VREG ? QN : 1];
     const int n3 = (NAMAX > 0 && (flags & kAtoms)) ? 3 * m.natom : 0;
+    /* few-atom cells of the material held in the parameters */
+    const bool kpar = VREG && NAMAX <= 4 && m.ion_off == a.ion_k_off;
     if constexpr (NAMAX > 0) {
         if (n3) {
-            const R* qv = a.ion_coef + m.ion_off;
             if constexpr (VREG) {
 #pragma unroll
-                for (int q = 0; q < QN; ++q)
-                    if (q < n3) {
-                        rold[q] = a.r[(int64_t)q * ns + slot];
-                        vold[q] = a.v[(int64_t)q * ns + slot];
-                    }
+                for (int q = 0; q < QN; ++q) {
+                    rold[q] = q < n3 ? a.r[(int64_t)q * ns + slot] : R(0);
+                    vold[q] = q < n3 ? a.v[(int64_t)q * ns + slot] : R(0);
+                }
             }
-            for_atoms<QN, VREG>(n3, [&](int q) {
-                R rq;
-                if constexpr (VREG) {
-                    rq = rold[q];
-                } else {
-                    rq = a.r[(int64_t)q * ns + slot];
-                    rold[q] = rq;
-                    /* v is read after E^{n+1}: bring it into L1 now */
-                    asm volatile("prefetch.global.L1 [%0];" ::"l"(a.v + (int64_t)q * ns + slot));
-                }
-                const int at = q / 3, d = q - 3 * at;
-                const R q0 = ldg(qv + at * 9 + 0 * 3 + d);
-                const R q1 = ldg(qv + at * 9 + 1 * 3 + d);
-                const R q2 = ldg(qv + at * 9 + 2 * 3 + d);
-                if constexpr (STRICT) {
-                    pr0 = SOp::add(pr0, SOp::mul(q0, rq));
-                    pr1 = SOp::add(pr1, SOp::mul(q1, rq));
-                    pr2 = SOp::add(pr2, SOp::mul(q2, rq));
-                } else {
-                    pr0 += q0 * rq;
-                    pr1 += q1 * rq;
-                    pr2 += q2 * rq;
-                }
-            });
+            auto ion_pr = [&](const auto& C) {
+                for_atoms<QN, VREG>(n3, [&](int q) {
+                    R rq;
+                    if constexpr (VREG) {
+                        rq = rold[q];
+                    } else {
+                        rq = a.r[(int64_t)q * ns + slot];
+                        rold[q] = rq;
+                        /* v is read after E^{n+1}: bring it into L1 now */
+                        asm volatile("prefetch.global.L1 [%0];" ::"l"(a.v + (int64_t)q * ns + slot));
+                    }
+                    const int at = q / 3, d = q - 3 * at;
+                    const R q0 = C.zv(at * 9 + 0 * 3 + d);
+                    const R q1 = C.zv(at * 9 + 1 * 3 + d);
+                    const R q2 = C.zv(at * 9 + 2 * 3 + d);
+                    if constexpr (STRICT) {
+                        pr0 = SOp::add(pr0, SOp::mul(q0, rq));
+                        pr1 = SOp::add(pr1, SOp::mul(q1, rq));
+                        pr2 = SOp::add(pr2, SOp::mul(q2, rq));
+                    } else {
+                        pr0 += q0 * rq;
+                        pr1 += q1 * rq;
+                        pr2 += q2 * rq;
+                    }
+                });
+            };
+            if (kpar) ion_pr(IonCoefParam<R>{a});
+            else ion_pr(IonCoefGlobal<R>{a.ion_coef + m.ion_off, n3});
         }
     }
 
@@ -564,23 +598,20 @@ __device__ __forceinline__ void e_update(const StepArgs<R>& a, const MatCoef<R>&
     /* ions: a = QeZM . E^{n+1} - DMM . r^n; r += v dt + a dt^2/2; v += a dt
      * (fdtd.c:3507-3528), all in the crystal frame */
     if constexpr (NAMAX > 0) {
-        if (n3) {
-            const R* qm = a.ion_coef + m.ion_off + 3 * n3;
-            const R* dmm = qm + 3 * n3;
-            const R dt = R(a.dt);
+        const R dt = R(a.dt);
+        auto ion_eom = [&](const auto& C) {
             for_atoms<QN, VREG>(n3, [&](int q) {
                 const int at = q / 3, d = q - 3 * at;
-                const R m0 = ldg(qm + at * 9 + 0 * 3 + d);
-                const R m1 = ldg(qm + at * 9 + 1 * 3 + d);
-                const R m2 = ldg(qm + at * 9 + 2 * 3 + d);
-                const R* row = dmm + (int64_t)q * n3;
+                const R m0 = C.zm(at * 9 + 0 * 3 + d);
+                const R m1 = C.zm(at * 9 + 1 * 3 + d);
+                const R m2 = C.zm(at * 9 + 2 * 3 + d);
                 R acc;
                 if constexpr (STRICT) {
                     acc = SOp::add(SOp::add(SOp::mul(m0, na), SOp::mul(m1, nb)), SOp::mul(m2, nc));
-                    for_atoms<QN, VREG>(n3, [&](int p) { acc = SOp::sub(acc, SOp::mul(ldg(row + p), rold[p])); });
+                    for_atoms<QN, VREG>(n3, [&](int p) { acc = SOp::sub(acc, SOp::mul(C.dmm(q, p), rold[p])); });
                 } else {
                     acc = m0 * na + m1 * nb + m2 * nc;
-                    for_atoms<QN, VREG>(n3, [&](int p) { acc -= ldg(row + p) * rold[p]; });
+                    for_atoms<QN, VREG>(n3, [&](int p) { acc -= C.dmm(q, p) * rold[p]; });
                 }
                 const int64_t o = (int64_t)q * ns + slot;
                 R vq;
@@ -594,6 +625,10 @@ __device__ __forceinline__ void e_update(const StepArgs<R>& a, const MatCoef<R>&
                     a.v[o] = vq + acc * dt;
                 }
             });
+        };
+        if (n3) {
+            if (kpar) ion_eom(IonCoefParam<R>{a});
+            else ion_eom(IonCoefGlobal<R>{a.ion_coef + m.ion_off, n3});
         }
     }
 
@@ -617,9 +652,11 @@ __device__ __forceinline__ void e_cell_values(const StepArgs<R>& a, int i, int j
     const R* __restrict__ exp_ = a.f.ex;
     const R* __restrict__ eyp = a.f.ey;
     const R* __restrict__ ezp = a.f.ez;
+    /* plain isotropic cells take E = iso * D without the material record */
+    const R iso = (!STRICT && PHP_ISO_PARAM && sizeof(R) == 4 && mid < kIsoMats) ? a.iso[mid] : R(0);
     /* mcs: the block's shared-memory copy of the first kSmemMats records */
-    const MatCoef<R>& m = (mcs && mid < a.nmat) ? mcs[mid] : a.mc[mid];
-    const int flags = m.flags;
+    const MatCoef<R>* mp = iso != R(0) ? nullptr : ((mcs && mid < a.nmat) ? &mcs[mid] : &a.mc[mid]);
+    const int flags = mp ? mp->flags : kIso;
     R ex = R(0), ey = R(0), ez = R(0);
     if (flags & (kLossy | kAde)) { ex = exp_[c]; ey = eyp[c]; ez = ezp[c]; }
     /* FP32 sums this step's D increment on its own before adding it to D:
@@ -635,7 +672,7 @@ __device__ __forceinline__ void e_cell_values(const StepArgs<R>& a, int i, int j
         else load_psi_d(a, i, j, k, sx, sy, ps);
         d_update<R, STRICT>(a, i, j, k, sx, sy, hx0, hy0, hz0, hxk, hyk, hz_jm, hx_jm, hz_im, hy_im, ps, ux, uy, uz);
         if (flags & kLossy) { /* fdtd.c:3349-3353 */
-            const R* q = m.eps_im;
+            const R* q = mp->eps_im;
             if constexpr (STRICT) {
                 dx = SOp::sub(dx, SOp::mul(SOp::mul(a.c1, SOp::add(SOp::add(SOp::mul(q[0], ex), SOp::mul(q[1], ey)), SOp::mul(q[2], ez))), a.eps0));
                 dy = SOp::sub(dy, SOp::mul(SOp::mul(a.c1, SOp::add(SOp::add(SOp::mul(q[3], ex), SOp::mul(q[4], ey)), SOp::mul(q[5], ez))), a.eps0));
@@ -669,7 +706,13 @@ __device__ __forceinline__ void e_cell_values(const StepArgs<R>& a, int i, int j
         dy += iy;
         dz += iz;
     }
-    e_update<R, STRICT, NAMAX>(a, m, c, dx, dy, dz, ix, iy, iz, ex, ey, ez);
+    if (!mp) {
+        ex = iso * dx;
+        ey = iso * dy;
+        ez = iso * dz;
+    } else {
+        e_update<R, STRICT, NAMAX>(a, *mp, c, dx, dy, dz, ix, iy, iz, ex, ey, ez);
+    }
     ex_out = ex;
     ey_out = ey;
     ez_out = ez;

@@ -2,7 +2,7 @@
  * fdtd_b200 -- drop-in replacement for PhP_FDTD's solver executable
  * (fdtd.x, fdtd.c:2075-4083) on one B200.
  *
- *   fdtd_b200 <config.cfg> [fp64|fp64-strict|fp32] [--spectra]
+ *   fdtd_b200 <config.cfg> [fp64|fp64-strict|fp32] [--spectra] [--sync-output]
  *
  * Reads the same .cfg, medium_map.bin and material files, prints the same
  * progress lines and writes the same output files as a single-rank run of
@@ -25,6 +25,8 @@
  * fdtd.c:3667), 2 bad input, 3 device failure.
  */
 #include <math.h>
+#include <pthread.h>
+#include <stdatomic.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -89,18 +91,188 @@ static void write_monitor_row(const php_cfg* cfg, FILE** f, int with_rv, int nat
     php_monitor_row(*f, step * cfg->dt, row, with_rv, r, v);
 }
 
+/* ------------------------------------------------------------ the writer
+ *
+ * The stepping thread enqueues a chunk of steps and its output frame
+ * (php_frame_begin) and goes on with the next chunk; the writer takes the
+ * frames in order, waits for each, writes what the reference writes at
+ * those steps (fdtd.c:3535-3883) and releases it.  The device is never idle
+ * for the writer's file output.  With --sync-output the stepping thread
+ * writes each frame itself before the next chunk. */
+
+typedef struct {
+    int t, next, n;  /* steps t .. next (n of them); t < 0 ends the writer */
+    int32_t ticket;
+} Item;
+
+#define WRITER_QUEUE (PHP_FRAME_SLOTS + 2)
+
+typedef struct {
+    const php_cfg* cfg;
+    php_ctx* ctx;
+    int nx, ny, nz;
+    int monitor_ok, monitor_rv, monitor_natom, full_ok, full_natom;
+    FILE *source_file, *monitor_file, *full_file;
+    double start;
+    atomic_int stop; /* divergence abort or failure: no further chunks */
+    int exit_code;
+    int dead;        /* after a stop: frames are waited for and released, nothing is written */
+    pthread_mutex_t mu;
+    pthread_cond_t cv;
+    Item q[WRITER_QUEUE];
+    int head, count;
+} Writer;
+
+static void writer_push(Writer* W, Item it)
+{
+    pthread_mutex_lock(&W->mu);
+    while (W->count == WRITER_QUEUE) pthread_cond_wait(&W->cv, &W->mu);
+    W->q[(W->head + W->count) % WRITER_QUEUE] = it;
+    W->count++;
+    pthread_cond_broadcast(&W->cv);
+    pthread_mutex_unlock(&W->mu);
+}
+
+static Item writer_pop(Writer* W)
+{
+    pthread_mutex_lock(&W->mu);
+    while (W->count == 0) pthread_cond_wait(&W->cv, &W->mu);
+    Item it = W->q[W->head];
+    W->head = (W->head + 1) % WRITER_QUEUE;
+    W->count--;
+    pthread_cond_broadcast(&W->cv);
+    pthread_mutex_unlock(&W->mu);
+    return it;
+}
+
+/* The divergence report of fdtd.c:3626-3668 from the frame's copy of the
+ * cell of max |r|. */
+static void report_divergence(Writer* W, const php_frame* fr, int last)
+{
+    const php_cfg* cfg = W->cfg;
+    const php_diag* dg = &fr->diag;
+    const int* am = dg->argmax_r;
+    printf("ERROR: r field too large at step %d\n", last);
+    printf("Max r value: %e\n", dg->max_r);
+    printf("Location: i=%d, j=%d, k=%d (global k=%d)\n", am[0], am[1], am[2], am[2]);
+    printf("Atom: %d, Direction: %d\n", am[3], am[4]);
+    const int idx = am[3] * 3 + am[4];
+    printf("v value: %e\n", fr->diag_v[idx]);
+    /* acceleration recomputed from the lab-frame E, as fdtd.c:3642-3663 */
+    const php_host_material* m = NULL;
+    int32_t* med = NULL;
+    char err[1024];
+    if (!php_medium_load(cfg->medium_file, W->nx, W->ny, W->nz, &med, err, sizeof(err))) {
+        m = &cfg->materials[med[((size_t)am[0] * W->ny + am[1]) * W->nz + am[2]]];
+        free(med);
+    }
+    if (m && m->qezm && m->dmm) {
+        double a_val = 0.0;
+        for (int iE = 0; iE < 3; iE++) a_val += m->qezm[am[3] * 9 + iE * 3 + am[4]] * fr->diag_point[iE];
+        for (int q = 0; q < 3 * m->natom; q++) a_val -= m->dmm[(size_t)idx * 3 * m->natom + q] * fr->diag_r[q];
+        printf("a value: %e\n", a_val);
+    }
+    fflush(stdout);
+}
+
+static void writer_item(Writer* W, const Item* it)
+{
+    const php_cfg* cfg = W->cfg;
+    php_frame fr;
+    int rc = php_frame_wait(W->ctx, it->ticket, &fr);
+    if (rc || W->dead) {
+        if (rc && !W->dead) {
+            W->exit_code = device_fail(W->ctx, "php_frame_wait", rc);
+            W->dead = 1;
+            atomic_store(&W->stop, 1);
+        }
+        php_frame_release(W->ctx, it->ticket);
+        return;
+    }
+    const int t = it->t, next = it->next, n = it->n;
+    /* source.txt rows of the output steps in this chunk (fdtd.c:3359-3400) */
+    for (int s = t; s <= next; s++) {
+        if (s % cfg->output_interval == 0 && W->source_file) {
+            double ct = s * cfg->dt;
+            fprintf(W->source_file, "%.4e  ", ct);
+            for (int q = 0; q < cfg->num_sources; q++) fprintf(W->source_file, "%.4e  ", php_source_value(&cfg->sources[q], ct));
+            fprintf(W->source_file, "\n");
+            fflush(W->source_file);
+        }
+    }
+    /* monitor rows (every step, fdtd.c:3806-3883): the row of an output step
+     * follows that step's diagnostics, so a divergence abort there drops it,
+     * as in the reference */
+    const int nrows = fr.nrows, row_len = fr.row_len;
+    if (W->monitor_ok)
+        for (int q = 0; q < nrows && t + q < next; q++)
+            write_monitor_row(cfg, &W->monitor_file, W->monitor_rv, W->monitor_natom, t + q, fr.rows + (size_t)q * row_len);
+    const int last = next;
+    if (last % cfg->output_interval == 0) {
+        const php_diag* dg = &fr.diag;
+        double current_time = last * cfg->dt;
+        printf("it %d/%d (%.1f%%), t = %.5e s,|E|_max = %.2e V/m,", last, cfg->tsteps, 100.0 * last / cfg->tsteps, current_time,
+               dg->max_e);
+        printf("r_max = %.2e A,", dg->max_r / 1e-10);
+        if (last > 0) {
+            double el = wall() - W->start;
+            double eta = el / last * (cfg->tsteps - last);
+            int eh = (int)(el / 3600), em = (int)((el - eh * 3600) / 60), es = (int)(el - eh * 3600 - em * 60);
+            int rh = (int)(eta / 3600), rm = (int)((eta - rh * 3600) / 60), rs = (int)(eta - rh * 3600 - rm * 60);
+            printf(" elapsed: %03d:%02d:%02d, ETA: %03d:%02d:%02d", eh, em, es, rh, rm, rs);
+        }
+        printf("\n");
+        fflush(stdout);
+        if (dg->max_r > 1e-10) { /* fdtd.c:3626-3668 */
+            report_divergence(W, &fr, last);
+            W->exit_code = 1;
+            W->dead = 1;
+            atomic_store(&W->stop, 1);
+            php_frame_release(W->ctx, it->ticket);
+            return;
+        }
+        if (fr.slice) {
+            char name[256];
+            php_slice_filename(name, sizeof(name), (char)cfg->output_slice_axis, cfg->output_slice_position, last);
+            php_write_slice_file(name, (char)cfg->output_slice_axis, W->nx, W->ny, W->nz, fr.slice);
+        }
+        if (W->full_ok) {
+            if (last == 0) {
+                W->full_file = fopen(cfg->full_monitor_output_file, "w");
+                if (W->full_file) php_full_monitor_header(W->full_file, W->full_natom);
+            }
+            if (W->full_file) php_full_monitor_row(W->full_file, current_time, fr.point, W->full_natom, fr.cell_r, fr.cell_v);
+        }
+    }
+    if (W->monitor_ok && nrows == n)
+        write_monitor_row(cfg, &W->monitor_file, W->monitor_rv, W->monitor_natom, next, fr.rows + (size_t)(n - 1) * row_len);
+    php_frame_release(W->ctx, it->ticket);
+}
+
+static void* writer_main(void* arg)
+{
+    Writer* W = (Writer*)arg;
+    for (;;) {
+        Item it = writer_pop(W);
+        if (it.t < 0) break;
+        writer_item(W, &it);
+    }
+    return NULL;
+}
+
 int main(int argc, char** argv)
 {
     printf("FDTD (B200) running on 1 GPU\n");
     if (argc < 2) {
-        printf("Usage: %s <config_file.cfg> [fp64|fp64-strict|fp32] [--spectra]\n", argv[0]);
+        printf("Usage: %s <config_file.cfg> [fp64|fp64-strict|fp32] [--spectra] [--sync-output]\n", argv[0]);
         return 1;
     }
     int precision = PHP_PREC_FP64;
-    int spectra = 0;
+    int spectra = 0, sync_output = 0;
     const char* pa = getenv("PHP_PRECISION");
     for (int a = 2; a < argc; a++) {
         if (!strcmp(argv[a], "--spectra")) spectra = 1;
+        else if (!strcmp(argv[a], "--sync-output")) sync_output = 1;
         else pa = argv[a];
     }
     if (pa) {
@@ -195,113 +367,77 @@ int main(int argc, char** argv)
         }
     }
 
-    FILE* source_file = fopen("source.txt", "w");
-    if (!source_file) fprintf(stderr, "Error opening source.txt for writing\n");
-    FILE* monitor_file = NULL;
-    FILE* full_file = NULL;
-    const int comp = php_component_from_name(cfg->output_component);
-    const char axis = cfg->output_slice_axis;
-    const int spos = cfg->output_slice_position;
-    size_t slice_n = axis == 'z' ? (size_t)nx * ny : axis == 'x' ? (size_t)ny * nz : (size_t)nx * nz;
-    float* slice = (float*)malloc(slice_n * sizeof(float));
-    const int max_rows = cfg->output_interval + 1;
-    double* rows = (double*)malloc((size_t)max_rows * (9 + 6 * (monitor_natom > 0 ? monitor_natom : 1)) * sizeof(double));
-    double* rv = (double*)malloc(sizeof(double) * 6 * (full_natom > 0 ? full_natom : 1));
+    Writer W;
+    memset(&W, 0, sizeof(W));
+    W.cfg = cfg;
+    W.ctx = ctx;
+    W.nx = nx;
+    W.ny = ny;
+    W.nz = nz;
+    W.monitor_ok = monitor_ok;
+    W.monitor_rv = monitor_rv;
+    W.monitor_natom = monitor_natom;
+    W.full_ok = full_ok;
+    W.full_natom = full_natom;
+    W.source_file = fopen("source.txt", "w");
+    if (!W.source_file) fprintf(stderr, "Error opening source.txt for writing\n");
+    pthread_mutex_init(&W.mu, NULL);
+    pthread_cond_init(&W.cv, NULL);
 
-    const double start = wall();
+    W.start = wall();
     printf("Entering iteration:\n");
     fflush(stdout);
+    pthread_t writer;
+    const int threaded = !sync_output && pthread_create(&writer, NULL, writer_main, &W) == 0;
     int t = 0;
     int exit_code = 0;
-    while (t < cfg->tsteps) {
+    while (t < cfg->tsteps && !atomic_load(&W.stop)) {
         /* run to the next output step (t % output_interval == 0) inclusive */
         int next = (t % cfg->output_interval == 0) ? t : (t / cfg->output_interval + 1) * cfg->output_interval;
         if (next > cfg->tsteps - 1) next = cfg->tsteps - 1;
         const int n = next - t + 1;
         if ((rc = php_step(ctx, n))) { exit_code = device_fail(ctx, "php_step", rc); break; }
-        /* source.txt rows of the output steps in this chunk (fdtd.c:3359-3400) */
-        for (int s = t; s <= next; s++) {
-            if (s % cfg->output_interval == 0 && source_file) {
-                double ct = s * cfg->dt;
-                fprintf(source_file, "%.4e  ", ct);
-                for (int q = 0; q < cfg->num_sources; q++) fprintf(source_file, "%.4e  ", php_source_value(&cfg->sources[q], ct));
-                fprintf(source_file, "\n");
-                fflush(source_file);
-            }
+        /* the frame of this chunk: probe rows of every step, and at an output
+         * step the diagnostics, the slice and the full-monitor cell */
+        const int out = next % cfg->output_interval == 0;
+        php_frame_req q;
+        memset(&q, 0, sizeof(q));
+        q.diag = out;
+        q.slice_comp = out ? php_component_from_name(cfg->output_component) : -1;
+        q.slice_axis = cfg->output_slice_axis;
+        q.slice_pos = cfg->output_slice_position;
+        q.probe = monitor_ok;
+        q.point[0] = q.cell[0] = -1;
+        if (out && full_ok) {
+            q.point[0] = q.cell[0] = cfg->monitor_x;
+            q.point[1] = q.cell[1] = cfg->monitor_y;
+            q.point[2] = cfg->monitor_z + 1;
+            q.cell[2] = cfg->monitor_z;
         }
-        /* monitor rows (every step, fdtd.c:3806-3883): the row of an output
-         * step follows that step's diagnostics, so a divergence abort there
-         * drops it, as in the reference */
-        int nrows = 0, row_len = 0;
-        if (monitor_ok) {
-            if ((rc = php_probe_read(ctx, rows, max_rows, &nrows, &row_len))) { exit_code = device_fail(ctx, "php_probe_read", rc); break; }
-            for (int q = 0; q < nrows && t + q < next; q++) write_monitor_row(cfg, &monitor_file, monitor_rv, monitor_natom, t + q, rows + (size_t)q * row_len);
+        Item it = {t, next, n, -1};
+        if ((rc = php_frame_begin(ctx, &q, &it.ticket))) {
+            if (q.slice_comp >= 0 && rc == PHP_ERR_INPUT) {
+                /* a slice the reference refuses (message, no file): the rest of the frame */
+                fprintf(stderr, "%s\n", php_last_error(ctx));
+                q.slice_comp = -1;
+                rc = php_frame_begin(ctx, &q, &it.ticket);
+            }
+            if (rc) { exit_code = device_fail(ctx, "php_frame_begin", rc); break; }
         }
-        const int last = next;
-        if (last % cfg->output_interval == 0) {
-            php_diag dg;
-            if ((rc = php_diagnostics(ctx, &dg))) { exit_code = device_fail(ctx, "php_diagnostics", rc); break; }
-            double current_time = last * cfg->dt;
-            printf("it %d/%d (%.1f%%), t = %.5e s,|E|_max = %.2e V/m,", last, cfg->tsteps, 100.0 * last / cfg->tsteps, current_time,
-                   dg.max_e);
-            printf("r_max = %.2e A,", dg.max_r / 1e-10);
-            if (last > 0) {
-                double el = wall() - start;
-                double eta = el / last * (cfg->tsteps - last);
-                int eh = (int)(el / 3600), em = (int)((el - eh * 3600) / 60), es = (int)(el - eh * 3600 - em * 60);
-                int rh = (int)(eta / 3600), rm = (int)((eta - rh * 3600) / 60), rs = (int)(eta - rh * 3600 - rm * 60);
-                printf(" elapsed: %03d:%02d:%02d, ETA: %03d:%02d:%02d", eh, em, es, rh, rm, rs);
-            }
-            printf("\n");
-            fflush(stdout);
-            if (dg.max_r > 1e-10) { /* fdtd.c:3626-3668 */
-                const int* am = dg.argmax_r;
-                printf("ERROR: r field too large at step %d\n", last);
-                printf("Max r value: %e\n", dg.max_r);
-                printf("Location: i=%d, j=%d, k=%d (global k=%d)\n", am[0], am[1], am[2], am[2]);
-                printf("Atom: %d, Direction: %d\n", am[3], am[4]);
-                int na = 0;
-                double rr[192], vv[192], e9[9];
-                php_read_cell_state(ctx, am[0], am[1], am[2], &na, rr, vv, NULL, NULL);
-                php_read_point(ctx, am[0], am[1], am[2], e9);
-                int idx = am[3] * 3 + am[4];
-                printf("v value: %e\n", vv[idx]);
-                /* acceleration recomputed from the lab-frame E, as fdtd.c:3642-3663 */
-                const php_host_material* m = NULL;
-                int32_t* med = NULL;
-                if (!php_medium_load(cfg->medium_file, nx, ny, nz, &med, err, sizeof(err))) {
-                    m = &cfg->materials[med[((size_t)am[0] * ny + am[1]) * nz + am[2]]];
-                    free(med);
-                }
-                if (m && m->qezm && m->dmm) {
-                    double a_val = 0.0;
-                    for (int iE = 0; iE < 3; iE++) a_val += m->qezm[am[3] * 9 + iE * 3 + am[4]] * e9[iE];
-                    for (int q = 0; q < 3 * m->natom; q++) a_val -= m->dmm[(size_t)idx * 3 * m->natom + q] * rr[q];
-                    printf("a value: %e\n", a_val);
-                }
-                fflush(stdout);
-                exit_code = 1;
-                break;
-            }
-            char name[256];
-            php_slice_filename(name, sizeof(name), axis, spos, last);
-            if (php_read_slice(ctx, comp, axis, spos, slice) == PHP_OK) php_write_slice_file(name, axis, nx, ny, nz, slice);
-            else fprintf(stderr, "%s\n", php_last_error(ctx));
-            if (full_ok) {
-                double e9[9];
-                int na = 0;
-                php_read_point(ctx, cfg->monitor_x, cfg->monitor_y, cfg->monitor_z + 1, e9);
-                php_read_cell_state(ctx, cfg->monitor_x, cfg->monitor_y, cfg->monitor_z, &na, rv, rv + 3 * full_natom, NULL, NULL);
-                if (last == 0) {
-                    full_file = fopen(cfg->full_monitor_output_file, "w");
-                    if (full_file) php_full_monitor_header(full_file, full_natom);
-                }
-                if (full_file) php_full_monitor_row(full_file, current_time, e9, full_natom, rv, rv + 3 * full_natom);
-            }
-        }
-        if (monitor_ok && nrows == n) write_monitor_row(cfg, &monitor_file, monitor_rv, monitor_natom, next, rows + (size_t)(n - 1) * row_len);
+        if (threaded) writer_push(&W, it);
+        else writer_item(&W, &it);
         t = next + 1;
     }
+    if (threaded) {
+        Item end = {-1, -1, 0, -1};
+        writer_push(&W, end);
+        pthread_join(writer, NULL);
+    }
+    if (W.exit_code && !exit_code) exit_code = W.exit_code;
+    FILE* source_file = W.source_file;
+    FILE* monitor_file = W.monitor_file;
+    FILE* full_file = W.full_file;
+    const double start = W.start;
     php_sync(ctx);
     if (spectra_id >= 0 && exit_code == 0) {
         double* acc = (double*)malloc(sizeof(double) * 2 * (size_t)spectra_count * nx * ny);
@@ -336,9 +472,8 @@ int main(int argc, char** argv)
         printf("Full monitor data saved to %s\n", cfg->full_monitor_output_file);
     }
     if (exit_code == 0) printf("\nSimulation completed in %.2f seconds\n", wall() - start);
-    free(slice);
-    free(rows);
-    free(rv);
+    pthread_mutex_destroy(&W.mu);
+    pthread_cond_destroy(&W.cv);
     php_destroy(ctx);
     php_cfg_free(cfg);
     return exit_code;

@@ -899,5 +899,7 @@ uint64_t php_host_sizeof(const char* n)
     if (!strcmp(n, "php_dft_request")) return sizeof(php_dft_request);
     if (!strcmp(n, "php_job_info")) return sizeof(php_job_info);
     if (!strcmp(n, "php_server_stats")) return sizeof(php_server_stats);
+    if (!strcmp(n, "php_frame_req")) return sizeof(php_frame_req);
+    if (!strcmp(n, "php_frame")) return sizeof(php_frame);
     return 0;
 }

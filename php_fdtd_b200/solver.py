@@ -318,6 +318,46 @@ class Simulation:
                                           C.byref(rl)))
         return buf[: n.value * rl.value].reshape(n.value, rl.value).copy()
 
+    def frame_begin(self, diag: bool = False, slice=None, probe: bool = False, point=None, cell=None) -> int:
+        """Enqueues an output frame behind the steps enqueued so far
+        (php_frame_begin) and returns its ticket at once.  slice is
+        (component, axis, position); point and cell are (i, j, k)."""
+        q = _abi.FrameReq()
+        q.diag = int(bool(diag))
+        q.slice_comp = -1
+        if slice is not None:
+            comp, axis, pos = slice
+            q.slice_comp, q.slice_axis, q.slice_pos = _comp(comp), ord(axis), int(pos)
+        q.probe = int(bool(probe))
+        q.point[:] = tuple(point) if point is not None else (-1, 0, 0)
+        q.cell[:] = tuple(cell) if cell is not None else (-1, 0, 0)
+        tk = C.c_int32()
+        self._ck(self._lib.php_frame_begin(self._ctx, C.byref(q), C.byref(tk)))
+        return tk.value
+
+    def frame_wait(self, ticket: int, release: bool = True) -> dict:
+        """Waits for frame `ticket` and returns copies of its parts
+        (php_frame_wait); releases the frame unless release is False."""
+        f = _abi.Frame()
+        try:
+            self._ck(self._lib.php_frame_wait(self._ctx, int(ticket), C.byref(f)))
+            out = {"step": f.step}
+            d = f.diag
+            out["diag"] = {"max_e": d.max_e, "max_ex": d.max_ex, "max_r": d.max_r, "argmax_r": tuple(d.argmax_r)}
+            n = 3 * f.diag_natom
+            out["diag_cell"] = {"natom": f.diag_natom, "point": np.array(f.diag_point[:]),
+                                "r": np.array(f.diag_r[:n]), "v": np.array(f.diag_v[:n])}
+            out["point"] = np.array(f.point[:])
+            n = 3 * f.cell_natom
+            out["cell"] = {"natom": f.cell_natom, "r": np.array(f.cell_r[:n]), "v": np.array(f.cell_v[:n])}
+            out["slice"] = (np.ctypeslib.as_array(f.slice, shape=(f.slice_len,)).copy() if f.slice_len else None)
+            out["rows"] = (np.ctypeslib.as_array(f.rows, shape=(f.nrows * f.row_len,)).reshape(f.nrows, f.row_len).copy()
+                           if f.nrows else np.empty((0, f.row_len)))
+        finally:
+            if release:
+                self._lib.php_frame_release(self._ctx, int(ticket))
+        return out
+
     def dft_add(self, comp, z_plane: int, freqs: Sequence[float], first_step: int = 0, interval: int = 1,
                 cast_f32: bool = False) -> int:
         f = np.ascontiguousarray(np.asarray(freqs, dtype=np.float64))

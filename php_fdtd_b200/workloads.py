@@ -149,6 +149,7 @@ class CaseSpec:
     full_monitor: int = 0
     medium_fn: Optional[object] = None                    # (nx,ny,nz) -> int32 array
     files_fn: Optional[object] = None                     # (dir) -> None, writes data files
+    expect_abort: bool = False                            # the run ends in the divergence abort (exit 1)
 
 
 def write_case(spec: CaseSpec, out: Path) -> Path:
@@ -275,6 +276,13 @@ _add(CaseSpec("ions2", 16, 16, 16, 60, pml=4, output_component="Ez", slice_pos=5
               sources=[_dip(8, 8, 11, wn=1370, t0=2e-16, tau=1e-16)], materials=[MAT_IONS2, MAT_IONS2_ROT],
               medium_fn=_blocks((0, 15, 0, 15, 0, 5, 8), (4, 11, 4, 11, 6, 7, 9)), files_fn=_all_files,
               monitor="x=8,y=8,z=4,atom=1,dir=z"))
+# ions2 driven hard enough that |r| passes 1e-10 m at step 20: the
+# reference's divergence report and abort (fdtd.c:3626-3668)
+_add(CaseSpec("ions2_diverge", 16, 16, 16, 60, pml=4, output_component="Ez", slice_pos=5,
+              sources=[_dip(8, 8, 11, wn=1370, t0=2e-16, tau=1e-16).replace("amplitude=1.0", "amplitude=1e24")],
+              materials=[MAT_IONS2, MAT_IONS2_ROT],
+              medium_fn=_blocks((0, 15, 0, 15, 0, 5, 8), (4, 11, 4, 11, 6, 7, 9)), files_fn=_all_files,
+              monitor="x=8,y=8,z=4,atom=1,dir=z", expect_abort=True))
 _add(CaseSpec("ions16", 14, 13, 12, 40, pml=3, output_component="Ey", slice_pos=4,
               sources=[_dip(7, 6, 9, c="x", wn=820, t0=2e-16, tau=1e-16)], materials=[MAT_IONS16],
               medium_fn=_blocks((2, 11, 2, 10, 1, 5, 10)), files_fn=_all_files,
