@@ -136,6 +136,7 @@ struct php_ctx {
     int ion_np = 0;              /* 3N padded to 16 */
     void* Pr = nullptr;          /* [3][nslot] */
     void* ion_dmm = nullptr;     /* CUDA-core kernel: [np][np] R */
+    void* ion_dfrag = nullptr;   /* FP64 ring: m8n8k4 B fragments */
     void* ion_bsplit = nullptr;  /* tensor kernel: DMM hi, lo bf16 images */
     bool ion_pipe = false;       /* TMA-fed pass (ion_pipe) */
     IonMaps ion_maps;
@@ -571,6 +572,7 @@ static void launch_ions(php_ctx* ctx)
     a.mc = (const MatCoef<R>*)ctx->mc;
     a.ion_coef = (const R*)ctx->ion_coef;
     a.dmm = (const R*)ctx->ion_dmm;
+    a.dfrag = (const double*)ctx->ion_dfrag;
     a.bsplit = (const uint32_t*)ctx->ion_bsplit;
     a.nslot = ctx->nslot;
     a.ntiles = (int32_t)((ctx->nslot + kIonTile - 1) / kIonTile);
@@ -933,6 +935,17 @@ static int setup_ion_pass(php_ctx* ctx, const std::vector<MatD>& mats, const std
             for (int p = 0; p < n3; p++) pad[(size_t)q * np + p] = D[(size_t)q * n3 + p];
         if ((rc = dalloc(ctx, &ctx->ion_dmm, pad.size() * sizeof(double)))) return rc;
         CK(cudaMemcpyAsync(ctx->ion_dmm, pad.data(), pad.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        /* the same matrix as B fragments of the m8n8k4 FP64 MMA (B[k][n] =
+         * DMM[n][k]): lane l of fragment (ks, nt) holds B[4 ks + l % 4][8 nt + l / 4] */
+        std::vector<double> frag((size_t)np * np, 0.0);
+        for (int ks = 0; ks < np / 4; ks++)
+            for (int nt = 0; nt < np / 8; nt++)
+                for (int l = 0; l < 32; l++) {
+                    const int q = nt * 8 + l / 4, p = ks * 4 + l % 4;
+                    frag[((size_t)ks * (np / 8) + nt) * 32 + l] = (q < n3 && p < n3) ? D[(size_t)q * n3 + p] : 0.0;
+                }
+        if ((rc = dalloc(ctx, &ctx->ion_dfrag, frag.size() * sizeof(double)))) return rc;
+        CK(cudaMemcpyAsync(ctx->ion_dfrag, frag.data(), frag.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
     }
     ctx->ion_np = np;

@@ -47,6 +47,7 @@ struct IonArgs {
     const MatCoef<R>* mc;
     const R* ion_coef;
     const R* dmm;                /* [NP][NP], zero padded (CUDA-core kernel) */
+    const double* dfrag;         /* FP64 ring: DMM as m8n8k4 B fragments [NP/4][NP/8][32 lanes] */
     const uint32_t* bsplit;      /* DMM hi, lo as bf16 in the UMMA K-major layout (tensor kernel) */
     int64_t nslot;
     int32_t ntiles;
@@ -185,7 +186,13 @@ __host__ __device__ constexpr int ion_cols() { return NP <= 32 ? 32 : 64; }
 template <typename R, int NP, int S>
 struct IonPipe {
     static constexpr bool TC = sizeof(R) == 4;
-    static constexpr int GROUPS = 2, CONSUMERS = GROUPS * kIonTile, THREADS = CONSUMERS + 32;
+    /* consumer groups: FP32 two groups of 128 threads take alternate tiles
+     * (one accumulator row per thread); FP64 one group of 256 threads takes
+     * each tile, so that with two stages one tile loads while one computes */
+    static constexpr int CONSUMERS = 2 * kIonTile, THREADS = CONSUMERS + 32;
+    static constexpr int GT = TC ? kIonTile : 2 * kIonTile, GROUPS = CONSUMERS / GT;
+    static constexpr int CELLS_PER_WARP = kIonTile / (GT / 32);  /* FP64: 16 */
+    static_assert(CONSUMERS % GT == 0 && GT % kIonTile == 0 && CELLS_PER_WARP % 16 == 0, "consumer layout");
     static constexpr uint32_t BOX = kIonTile * NP * sizeof(R);      /* one array's tile, NP rows */
     /* per stage: r, v, then the slots' cell offsets (int64, 1024 B), atom
      * coordinate counts (int32, 512 B) and material ids (uint8, 128 B) */
@@ -243,6 +250,16 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar)
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
+/* D += A B for one 8 x 8 x 4 FP64 tile (the FP64 tensor path): per lane
+ * g = lane / 4, t = lane % 4, a = A[g][t], b = B[t][g], and c0, c1 =
+ * C[g][2t], C[g][2t + 1] */
+__device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
 /* B-byte asynchronous copy global -> shared (B = 4, 8 or 16) */
 template <int B>
 __device__ __forceinline__ void cp_async_ca(void* dst, const void* src)
@@ -281,7 +298,7 @@ __global__ void __launch_bounds__(IonPipe<R, NP, S>::THREADS, 1)
     /* DMM (bf16 images for the tensor cores, or the padded FP64 matrix) and
      * the lattice's QeZV, QeZM (cells of other materials read global) */
     {
-        const uint4* src = P::TC ? reinterpret_cast<const uint4*>(a.bsplit) : reinterpret_cast<const uint4*>(a.dmm);
+        const uint4* src = P::TC ? reinterpret_cast<const uint4*>(a.bsplit) : reinterpret_cast<const uint4*>(a.dfrag);
         unsigned char* dst0 = P::TC ? ops + P::GROUPS * 2 * P::A_BYTES : ops;
         const int n16 = (int)((P::TC ? 2 * P::B_BYTES : NP * NP * sizeof(R)) / 16);
         uint4* dst = reinterpret_cast<uint4*>(dst0);
@@ -313,7 +330,7 @@ __global__ void __launch_bounds__(IonPipe<R, NP, S>::THREADS, 1)
     const uint32_t tx_bytes = 2u * kIonTile * (uint32_t)n3 * (uint32_t)sizeof(R);
     bool failed = false;
 
-    if (warp == P::GROUPS * 4) {
+    if (warp == P::CONSUMERS / 32) {
         /* ------------------------------------------------------ producer */
         const int lane = tid & 31;
         int issued = 0;
@@ -361,28 +378,30 @@ __global__ void __launch_bounds__(IonPipe<R, NP, S>::THREADS, 1)
         }
     } else {
         /* ------------------------------------------------------ consumers */
-        const int g = warp >> 2, gt = tid & (kIonTile - 1), bar_id = 1 + g;
+        const int g = tid / P::GT, gi = tid % P::GT, gt = gi & (kIonTile - 1), bar_id = 1 + g;
+        /* FP64: threads gi >= 128 take part in the contraction only */
+        const bool cell_thread = gi < kIonTile;
         const int64_t ns = a.nslot;
         const R dt = R(a.dt);
         unsigned char* Ahi = ops + g * 2 * P::A_BYTES;
         unsigned char* Alo = Ahi + P::A_BYTES;
         const unsigned char* Bhi = ops + P::GROUPS * 2 * P::A_BYTES;
         const unsigned char* Blo = Bhi + P::B_BYTES;
-        const R* Dsm = reinterpret_cast<const R*>(ops);
+        const double* Bfrag = reinterpret_cast<const double*>(ops);
         const uint32_t tmem = tmem0 + (uint32_t)(g * ion_cols<NP>());
         uint32_t mphase = 0;
         for (int k = g; k < mine; k += P::GROUPS) {
             const int st = k % S;
             const int64_t s = (int64_t)((int)blockIdx.x + k * (int)gridDim.x) * kIonTile + gt;
             const bool got = mbar_wait(&full[st], (k / S) & 1);
-            if (named_sync_or(bar_id, kIonTile, !got)) {
+            if (named_sync_or(bar_id, P::GT, !got)) {
                 failed = true;
                 break;
             }
             unsigned char* sb = stages + st * P::STAGE;
             R* rs = reinterpret_cast<R*>(sb);
             R* vs = reinterpret_cast<R*>(sb + P::BOX);
-            const int n3c = s < ns ? reinterpret_cast<const int32_t*>(sb + 2 * P::BOX + 1024)[gt] : 0;
+            const int n3c = (cell_thread && s < ns) ? reinterpret_cast<const int32_t*>(sb + 2 * P::BOX + 1024)[gt] : 0;
             R e0 = R(0), e1 = R(0), e2 = R(0);
             const MatCoef<R>* mp = nullptr;
             if (n3c) {
@@ -418,7 +437,7 @@ __global__ void __launch_bounds__(IonPipe<R, NP, S>::THREADS, 1)
                 }
                 fence_proxy_async_smem();
                 asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-                named_sync(bar_id, kIonTile);
+                named_sync(bar_id, P::GT);
                 if (gt == 0) {
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                     const uint32_t idesc = umma_idesc_bf16(kIonTile, NP);
@@ -448,12 +467,16 @@ __global__ void __launch_bounds__(IonPipe<R, NP, S>::THREADS, 1)
                 }
                 const bool done = mbar_wait(&mma_bar[g], mphase);
                 mphase ^= 1u;
-                if (named_sync_or(bar_id, kIonTile, !done)) {
+                if (named_sync_or(bar_id, P::GT, !done)) {
                     failed = true;
                     if (gt == 0) mbar_wait(&mma_bar[g], mphase ^ 1u); /* the MMAs in flight finish first */
                     break;
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                /* epilogue with the coefficients from shared memory when every
+                 * cell of the warp has the lattice's, else through qv, qm (the
+                 * choice is warp-uniform: tcgen05.ld is warp-collective) */
+                auto epilogue = [&](const R* zv, const R* zm) {
 #pragma unroll
                 for (int cb = 0; cb < NP; cb += 16) {
                     uint32_t d[16];
@@ -469,67 +492,119 @@ __global__ void __launch_bounds__(IonPipe<R, NP, S>::THREADS, 1)
                         const int q = cb + u;
                         if (q < n3c) {
                             const int at = q / 3, dd = q - 3 * at;
-                            const R acc = qm[at * 9 + dd] * e0 + qm[at * 9 + 3 + dd] * e1 + qm[at * 9 + 6 + dd] * e2 -
+                            const R acc = zm[at * 9 + dd] * e0 + zm[at * 9 + 3 + dd] * e1 + zm[at * 9 + 6 + dd] * e2 -
                                           __uint_as_float(d[u]);
                             const int o = q * kIonTile + gt;
                             const R vq = vs[o];
                             const R rn = rs[o] + (vq * dt + R(0.5) * acc * dt * dt);
                             rs[o] = rn;
                             vs[o] = vq + acc * dt;
-                            p0 += qv[at * 9 + dd] * rn;
-                            p1 += qv[at * 9 + 3 + dd] * rn;
-                            p2 += qv[at * 9 + 6 + dd] * rn;
+                            p0 += zv[at * 9 + dd] * rn;
+                            p1 += zv[at * 9 + 3 + dd] * rn;
+                            p2 += zv[at * 9 + 6 + dd] * rn;
                         }
                     }
                 }
+                };
+                const bool lattice = !n3c || mp->ion_off == a.ion_off_ref;
+                if (__all_sync(0xffffffffu, lattice)) epilogue(coef, coef + 3 * n3c);
+                else epilogue(qv, qm);
                 asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             } else {
-                R rold[NP];
-#pragma unroll
-                for (int q = 0; q < NP; ++q) rold[q] = q < n3 ? rs[q * kIonTile + gt] : R(0);
-                /* QG independent accumulation chains; 288 threads leave 168
-                 * registers a thread, which four FP64 chains fit */
-                constexpr int QG = sizeof(R) == 8 ? 4 : 8;
+                /* FP64: DMM . r on the FP64 tensor path (mma.sync m8n8k4).
+                 * Each thread leaves its cell's crystal-frame E and the
+                 * offset of its QeZV, QeZM in the stage; then each warp
+                 * takes its 32 cells, 16 at a time: the accumulators hold
+                 * (DMM . r)[cell][q] for two 8-cell rows and all NP columns,
+                 * and the lanes that hold a (cell, q) pair update that
+                 * coordinate's r and v in the stage. */
+                R* es = reinterpret_cast<R*>(sb + P::E_OFF);
+                int64_t* qoff = reinterpret_cast<int64_t*>(sb + 2 * P::BOX); /* slot cells, no longer read */
+                const int32_t* n3s = reinterpret_cast<const int32_t*>(sb + 2 * P::BOX + 1024);
+                if (cell_thread) {
+                    es[gt] = e0;
+                    es[kIonTile + gt] = e1;
+                    es[2 * kIonTile + gt] = e2;
+                    qoff[gt] = n3c ? (mp->ion_off == a.ion_off_ref ? -1 : (int64_t)mp->ion_off) : 0;
+                }
+                named_sync(bar_id, P::GT);
+                const int lane = tid & 31, grp = lane >> 2, tig = lane & 3;
+                const int64_t x0 = (int64_t)((int)blockIdx.x + k * (int)gridDim.x) * kIonTile;
 #pragma unroll 1
-                for (int q0 = 0; q0 < n3c; q0 += QG) {
-                    R acc[QG];
+                for (int pass = 0; pass < P::CELLS_PER_WARP / 16; ++pass) {
+                    const int cb = (gi >> 5) * P::CELLS_PER_WARP + pass * 16;
+                    double acc[2][NP / 8][2];
 #pragma unroll
-                    for (int u = 0; u < QG; ++u) {
-                        const int q = q0 + u;
-                        const int at = q / 3, dd = q - 3 * at;
-                        acc[u] = q < n3c ? qm[at * 9 + dd] * e0 + qm[at * 9 + 3 + dd] * e1 + qm[at * 9 + 6 + dd] * e2 : R(0);
-                    }
+                    for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
-                    for (int p = 0; p < NP; p += 2) {
+                        for (int nt = 0; nt < NP / 8; ++nt) acc[mt][nt][0] = acc[mt][nt][1] = 0.0;
+#pragma unroll 4
+                    for (int ks = 0; ks < NP / 4; ++ks) {
+                        const int kk = ks * 4 + tig;
+                        /* rows past 3N hold no data: A is zero there */
+                        const double a0 = kk < n3 ? (double)rs[kk * kIonTile + cb + grp] : 0.0;
+                        const double a1 = kk < n3 ? (double)rs[kk * kIonTile + cb + 8 + grp] : 0.0;
 #pragma unroll
-                        for (int u = 0; u < QG; ++u) {
-                            const R* dr = Dsm + min(q0 + u, NP - 1) * NP + p;
-                            if constexpr (sizeof(R) == 8) {
-                                const double2 d2 = *reinterpret_cast<const double2*>(dr);
-                                acc[u] -= d2.x * rold[p] + d2.y * rold[p + 1];
-                            } else {
-                                acc[u] -= dr[0] * rold[p] + dr[1] * rold[p + 1];
-                            }
+                        for (int nt = 0; nt < NP / 8; ++nt) {
+                            const double b = Bfrag[(ks * (NP / 8) + nt) * 32 + lane];
+                            dmma_8x8x4(acc[0][nt][0], acc[0][nt][1], a0, b);
+                            dmma_8x8x4(acc[1][nt][0], acc[1][nt][1], a1, b);
                         }
                     }
 #pragma unroll
-                    for (int u = 0; u < QG; ++u) {
-                        const int q = q0 + u;
-                        if (q < n3c) {
-                            const int at = q / 3, dd = q - 3 * at;
-                            const int o = q * kIonTile + gt;
-                            const R vq = vs[o];
-                            const R rn = rs[o] + (vq * dt + R(0.5) * acc[u] * dt * dt);
-                            rs[o] = rn;
-                            vs[o] = vq + acc[u] * dt;
-                            p0 += qv[at * 9 + dd] * rn;
-                            p1 += qv[at * 9 + 3 + dd] * rn;
-                            p2 += qv[at * 9 + 6 + dd] * rn;
+                    for (int mt = 0; mt < 2; ++mt) {
+                        const int cl = cb + 8 * mt + grp;
+                        const bool live = x0 + cl < ns;
+                        const int n3l = live ? n3s[cl] : 0;
+                        R q0 = R(0), q1 = R(0), q2 = R(0);
+                        /* the update with the lattice's coefficients from shared memory
+                         * (qo < 0) or another material's from global memory: two
+                         * copies, each with its loads in a known address space */
+                        auto update = [&](const R* zv) {
+                            const R ex0 = es[cl], ex1 = es[kIonTile + cl], ex2 = es[2 * kIonTile + cl];
+                            const R* zm = zv + 3 * n3l;
+#pragma unroll
+                            for (int nt = 0; nt < NP / 8; ++nt)
+#pragma unroll
+                                for (int j = 0; j < 2; ++j) {
+                                    const int q = nt * 8 + 2 * tig + j;
+                                    if (q < n3l) {
+                                        const int at = q / 3, dd = q - 3 * at;
+                                        const R acc_q = zm[at * 9 + dd] * ex0 + zm[at * 9 + 3 + dd] * ex1 +
+                                                        zm[at * 9 + 6 + dd] * ex2 - (R)acc[mt][nt][j];
+                                        const int o = q * kIonTile + cl;
+                                        const R vq = vs[o];
+                                        const R rn = rs[o] + (vq * dt + R(0.5) * acc_q * dt * dt);
+                                        rs[o] = rn;
+                                        vs[o] = vq + acc_q * dt;
+                                        q0 += zv[at * 9 + dd] * rn;
+                                        q1 += zv[at * 9 + 3 + dd] * rn;
+                                        q2 += zv[at * 9 + 6 + dd] * rn;
+                                    }
+                                }
+                        };
+                        if (n3l) {
+                            const int64_t qo = qoff[cl];
+                            if (qo < 0) update(coef);
+                            else update(a.ion_coef + qo);
+                        }
+                        /* P_ion of the cell: the sum over its four lanes */
+#pragma unroll
+                        for (int m = 1; m < 4; m <<= 1) {
+                            q0 += __shfl_xor_sync(0xffffffffu, q0, m);
+                            q1 += __shfl_xor_sync(0xffffffffu, q1, m);
+                            q2 += __shfl_xor_sync(0xffffffffu, q2, m);
+                        }
+                        if (n3l && tig == 0) {
+                            const int64_t sl = x0 + cl;
+                            a.pr[sl] = q0;
+                            a.pr[ns + sl] = q1;
+                            a.pr[2 * ns + sl] = q2;
                         }
                     }
                 }
             }
-            if (n3c) {
+            if (P::TC && n3c) {
                 a.pr[s] = p0;
                 a.pr[ns + s] = p1;
                 a.pr[2 * ns + s] = p2;
@@ -537,8 +612,8 @@ __global__ void __launch_bounds__(IonPipe<R, NP, S>::THREADS, 1)
             /* the updated tile goes back with one tensor store per array;
              * the stage is free once the store has read it */
             fence_proxy_async_smem();
-            named_sync(bar_id, kIonTile);
-            if (gt == 0) {
+            named_sync(bar_id, P::GT);
+            if (gi == 0) {
                 const int x = ((int)blockIdx.x + k * (int)gridDim.x) * kIonTile;
                 tma_store_3d(&maps.r, rs, x, 0, 0);
                 tma_store_3d(&maps.v, vs, x, 0, 0);
@@ -548,8 +623,8 @@ __global__ void __launch_bounds__(IonPipe<R, NP, S>::THREADS, 1)
                 mbar_arrive(&empty[st]);
             }
         }
-        if (failed && gt == 0) atomicExch(a.err, 1);
-        if (gt == 0) bulk_wait0(); /* stores complete before the CTA leaves */
+        if (failed && gi == 0) atomicExch(a.err, 1);
+        if (gi == 0) bulk_wait0(); /* stores complete before the CTA leaves */
     }
     if constexpr (P::TC) asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
