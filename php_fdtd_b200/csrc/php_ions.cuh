@@ -334,10 +334,24 @@ __global__ void __launch_bounds__(IonPipe<R, NP, S>::THREADS, 1)
         /* ------------------------------------------------------ producer */
         const int lane = tid & 31;
         int issued = 0;
+        /* lane 0: once the consumers are done with tile kk, its stage goes back
+         * with one tensor store per array (the consumers never wait for it) */
+        auto store_tile = [&](int kk) -> bool {
+            if (!mbar_wait(&empty[kk % S], (kk / S) & 1)) return false;
+            const int x = ((int)blockIdx.x + kk * (int)gridDim.x) * kIonTile;
+            unsigned char* b = stages + (kk % S) * P::STAGE;
+            tma_store_3d(&maps.r, b, x, 0, 0);
+            tma_store_3d(&maps.v, b + P::BOX, x, 0, 0);
+            bulk_commit();
+            return true;
+        };
         for (int k = 0; k < mine; ++k) {
             const int st = k % S;
             bool ok = true;
-            if (k >= S && lane == 0) ok = mbar_wait(&empty[st], ((k / S) - 1) & 1);
+            if (k >= S && lane == 0) {
+                ok = store_tile(k - S);
+                if (ok) bulk_wait_read0(); /* the stage is free once the store has read it */
+            }
             if (!__shfl_sync(0xffffffffu, ok ? 1 : 0, 0)) {
                 failed = true;
                 break;
@@ -371,11 +385,14 @@ __global__ void __launch_bounds__(IonPipe<R, NP, S>::THREADS, 1)
             cp_async_arrive_noinc(&full[st]);
             issued = k + 1;
         }
+        if (lane == 0 && !failed)
+            for (int kk = max(0, mine - S); kk < mine && !failed; ++kk) failed = !store_tile(kk);
         if (failed && lane == 0) {
             atomicExch(a.err, 1);
             /* loads issued and not consumed land before the CTA leaves */
             for (int k = *consumed; k < issued; ++k) mbar_wait(&full[k % S], (k / S) & 1);
         }
+        if (lane == 0) bulk_wait0(); /* stores complete before the CTA leaves */
     } else {
         /* ------------------------------------------------------ consumers */
         const int g = tid / P::GT, gi = tid % P::GT, gt = gi & (kIonTile - 1), bar_id = 1 + g;
@@ -609,22 +626,17 @@ __global__ void __launch_bounds__(IonPipe<R, NP, S>::THREADS, 1)
                 a.pr[ns + s] = p1;
                 a.pr[2 * ns + s] = p2;
             }
-            /* the updated tile goes back with one tensor store per array;
-             * the stage is free once the store has read it */
+            /* the updated tile is complete in the stage: the producer stores it
+             * (the writes are ordered before the tensor store's reads by the
+             * proxy fence, the barrier and the arrival) */
             fence_proxy_async_smem();
             named_sync(bar_id, P::GT);
             if (gi == 0) {
-                const int x = ((int)blockIdx.x + k * (int)gridDim.x) * kIonTile;
-                tma_store_3d(&maps.r, rs, x, 0, 0);
-                tma_store_3d(&maps.v, vs, x, 0, 0);
-                bulk_commit();
-                bulk_wait_read0();
                 atomicMax((int32_t*)consumed, k + 1);
                 mbar_arrive(&empty[st]);
             }
         }
         if (failed && gi == 0) atomicExch(a.err, 1);
-        if (gi == 0) bulk_wait0(); /* stores complete before the CTA leaves */
     }
     if constexpr (P::TC) asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
