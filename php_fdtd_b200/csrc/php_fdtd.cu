@@ -936,14 +936,29 @@ static int setup_ion_pass(php_ctx* ctx, const std::vector<MatD>& mats, const std
         if ((rc = dalloc(ctx, &ctx->ion_dmm, pad.size() * sizeof(double)))) return rc;
         CK(cudaMemcpyAsync(ctx->ion_dmm, pad.data(), pad.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
         /* the same matrix as B fragments of the m8n8k4 FP64 MMA (B[k][n] =
-         * DMM[n][k]): lane l of fragment (ks, nt) holds B[4 ks + l % 4][8 nt + l / 4] */
-        std::vector<double> frag((size_t)np * np, 0.0);
+         * DMM[n][k]): lane l of fragment (ks, nt) holds B[4 ks + l % 4][8 nt + l / 4];
+         * then the E step, B[t][q] = -QeZM(q, t) (t < 3), and P_ion's B[p][c] =
+         * QeZV(c, p) (c < 3), both of the lattice (fdtd.c:3418-3427, 3507-3528) */
+        const double* zv = d.materials[ref].qezv;
+        const double* zm = d.materials[ref].qezm;
+        std::vector<double> frag((size_t)np * np + (size_t)(np / 8) * 32 + (size_t)(np / 4) * 32, 0.0);
         for (int ks = 0; ks < np / 4; ks++)
             for (int nt = 0; nt < np / 8; nt++)
                 for (int l = 0; l < 32; l++) {
                     const int q = nt * 8 + l / 4, p = ks * 4 + l % 4;
                     frag[((size_t)ks * (np / 8) + nt) * 32 + l] = (q < n3 && p < n3) ? D[(size_t)q * n3 + p] : 0.0;
                 }
+        const size_t fe = (size_t)np * np, fp = fe + (size_t)(np / 8) * 32;
+        for (int nt = 0; nt < np / 8; nt++)
+            for (int l = 0; l < 32; l++) {
+                const int t = l % 4, q = nt * 8 + l / 4;
+                frag[fe + (size_t)nt * 32 + l] = (t < 3 && q < n3) ? -zm[(q / 3) * 9 + t * 3 + q % 3] : 0.0;
+            }
+        for (int ks = 0; ks < np / 4; ks++)
+            for (int l = 0; l < 32; l++) {
+                const int p = ks * 4 + l % 4, c = l / 4;
+                frag[fp + (size_t)ks * 32 + l] = (c < 3 && p < n3) ? zv[(p / 3) * 9 + c * 3 + p % 3] : 0.0;
+            }
         if ((rc = dalloc(ctx, &ctx->ion_dfrag, frag.size() * sizeof(double)))) return rc;
         CK(cudaMemcpyAsync(ctx->ion_dfrag, frag.data(), frag.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));

@@ -204,8 +204,11 @@ struct IonPipe {
     static constexpr uint32_t STAGE = 2 * BOX + IDX + EB;
     static constexpr uint32_t A_BYTES = kIonTile * NP * 2;           /* bf16 rows of one group */
     static constexpr uint32_t B_BYTES = NP * NP * 2;
-    static constexpr uint32_t OPS = TC ? GROUPS * 2 * A_BYTES + 2 * B_BYTES : NP * NP * sizeof(R);
-    static constexpr uint32_t COEF = 2 * 3 * NP * sizeof(R);         /* QeZV, QeZM: 9N each, 9N <= 3 NP */
+    /* FP64: DMM, -QeZM (the E step) and QeZV^T (P_ion) as m8n8k4 B fragments */
+    static constexpr uint32_t FRAG_E = NP * NP, FRAG_P = FRAG_E + (NP / 8) * 32, FRAG_N = FRAG_P + (NP / 4) * 32;
+    static constexpr uint32_t OPS = TC ? GROUPS * 2 * A_BYTES + 2 * B_BYTES : FRAG_N * 8;
+    /* FP32: the lattice's QeZV, QeZM (9N each, 9N <= 3 NP) */
+    static constexpr uint32_t COEF = TC ? 2 * 3 * NP * sizeof(R) : 0;
     static constexpr uint32_t SMEM = 1024 + S * STAGE + OPS + COEF + 256;
 };
 
@@ -300,10 +303,11 @@ __global__ void __launch_bounds__(IonPipe<R, NP, S>::THREADS, 1)
     {
         const uint4* src = P::TC ? reinterpret_cast<const uint4*>(a.bsplit) : reinterpret_cast<const uint4*>(a.dfrag);
         unsigned char* dst0 = P::TC ? ops + P::GROUPS * 2 * P::A_BYTES : ops;
-        const int n16 = (int)((P::TC ? 2 * P::B_BYTES : NP * NP * sizeof(R)) / 16);
+        const int n16 = (int)((P::TC ? 2 * P::B_BYTES : P::OPS) / 16);
         uint4* dst = reinterpret_cast<uint4*>(dst0);
         for (int t = tid; t < n16; t += P::THREADS) dst[t] = src[t];
-        for (int t = tid; t < 6 * n3; t += P::THREADS) coef[t] = a.ion_coef[a.ion_off_ref + t];
+        if constexpr (P::TC)
+            for (int t = tid; t < 6 * n3; t += P::THREADS) coef[t] = a.ion_coef[a.ion_off_ref + t];
     }
     if constexpr (P::TC) {
         if (warp == 0) {
@@ -550,6 +554,18 @@ __global__ void __launch_bounds__(IonPipe<R, NP, S>::THREADS, 1)
 #pragma unroll 1
                 for (int pass = 0; pass < P::CELLS_PER_WARP / 16; ++pass) {
                     const int cb = (gi >> 5) * P::CELLS_PER_WARP + pass * 16;
+                    int n3l[2];
+                    bool lat = true;
+#pragma unroll
+                    for (int mt = 0; mt < 2; ++mt) {
+                        const int cl = cb + 8 * mt + grp;
+                        n3l[mt] = x0 + cl < ns ? n3s[cl] : 0;
+                        lat = lat && (n3l[mt] == 0 || qoff[cl] < 0);
+                    }
+                    /* every cell of the 16 has the lattice's coefficients: QeZM . E
+                     * joins the contraction as one more k step and P_ion = QeZV . r
+                     * is a second contraction (warp-uniform choice) */
+                    const bool fold = __all_sync(0xffffffffu, lat);
                     double acc[2][NP / 8][2];
 #pragma unroll
                     for (int mt = 0; mt < 2; ++mt)
@@ -568,24 +584,76 @@ __global__ void __launch_bounds__(IonPipe<R, NP, S>::THREADS, 1)
                             dmma_8x8x4(acc[1][nt][0], acc[1][nt][1], a1, b);
                         }
                     }
+                    if (fold) {
+                        const double a0 = tig < 3 ? (double)es[tig * kIonTile + cb + grp] : 0.0;
+                        const double a1 = tig < 3 ? (double)es[tig * kIonTile + cb + 8 + grp] : 0.0;
+#pragma unroll
+                        for (int nt = 0; nt < NP / 8; ++nt) {
+                            const double b = Bfrag[P::FRAG_E + nt * 32 + lane];
+                            dmma_8x8x4(acc[0][nt][0], acc[0][nt][1], a0, b);
+                            dmma_8x8x4(acc[1][nt][0], acc[1][nt][1], a1, b);
+                        }
+                        /* acc = DMM . r - QeZM . E = -a */
+#pragma unroll
+                        for (int mt = 0; mt < 2; ++mt) {
+                            const int cl = cb + 8 * mt + grp;
+                            if (n3l[mt]) {
+#pragma unroll
+                                for (int nt = 0; nt < NP / 8; ++nt)
+#pragma unroll
+                                    for (int j = 0; j < 2; ++j) {
+                                        const int q = nt * 8 + 2 * tig + j;
+                                        if (q < n3) {
+                                            const R acc_q = -(R)acc[mt][nt][j];
+                                            const int o = q * kIonTile + cl;
+                                            const R vq = vs[o];
+                                            rs[o] = rs[o] + (vq * dt + R(0.5) * acc_q * dt * dt);
+                                            vs[o] = vq + acc_q * dt;
+                                        }
+                                    }
+                            }
+                        }
+                        __syncwarp();
+                        /* P_ion = QeZV . r^{n+1}: lanes t = 0, 1 of each cell hold
+                         * components 2t, 2t + 1 */
+                        double pa[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll 4
+                        for (int ks = 0; ks < NP / 4; ++ks) {
+                            const int kk = ks * 4 + tig;
+                            const double a0 = kk < n3 ? (double)rs[kk * kIonTile + cb + grp] : 0.0;
+                            const double a1 = kk < n3 ? (double)rs[kk * kIonTile + cb + 8 + grp] : 0.0;
+                            const double b = Bfrag[P::FRAG_P + ks * 32 + lane];
+                            dmma_8x8x4(pa[0][0], pa[0][1], a0, b);
+                            dmma_8x8x4(pa[1][0], pa[1][1], a1, b);
+                        }
+#pragma unroll
+                        for (int mt = 0; mt < 2; ++mt) {
+                            const int64_t sl = x0 + cb + 8 * mt + grp;
+                            if (n3l[mt] && tig == 0) {
+                                a.pr[sl] = (R)pa[mt][0];
+                                a.pr[ns + sl] = (R)pa[mt][1];
+                            }
+                            if (n3l[mt] && tig == 1) a.pr[2 * ns + sl] = (R)pa[mt][0];
+                        }
+                        continue;
+                    }
 #pragma unroll
                     for (int mt = 0; mt < 2; ++mt) {
                         const int cl = cb + 8 * mt + grp;
-                        const bool live = x0 + cl < ns;
-                        const int n3l = live ? n3s[cl] : 0;
                         R q0 = R(0), q1 = R(0), q2 = R(0);
-                        /* the update with the lattice's coefficients from shared memory
-                         * (qo < 0) or another material's from global memory: two
-                         * copies, each with its loads in a known address space */
-                        auto update = [&](const R* zv) {
+                        /* cells of several materials: QeZM . E and QeZV . r from
+                         * each cell's coefficients in global memory */
+                        if (n3l[mt]) {
+                            const int64_t qo = qoff[cl];
+                            const R* zv = a.ion_coef + (qo < 0 ? (int64_t)a.ion_off_ref : qo);
+                            const R* zm = zv + 3 * n3l[mt];
                             const R ex0 = es[cl], ex1 = es[kIonTile + cl], ex2 = es[2 * kIonTile + cl];
-                            const R* zm = zv + 3 * n3l;
 #pragma unroll
                             for (int nt = 0; nt < NP / 8; ++nt)
 #pragma unroll
                                 for (int j = 0; j < 2; ++j) {
                                     const int q = nt * 8 + 2 * tig + j;
-                                    if (q < n3l) {
+                                    if (q < n3l[mt]) {
                                         const int at = q / 3, dd = q - 3 * at;
                                         const R acc_q = zm[at * 9 + dd] * ex0 + zm[at * 9 + 3 + dd] * ex1 +
                                                         zm[at * 9 + 6 + dd] * ex2 - (R)acc[mt][nt][j];
@@ -599,11 +667,6 @@ __global__ void __launch_bounds__(IonPipe<R, NP, S>::THREADS, 1)
                                         q2 += zv[at * 9 + 6 + dd] * rn;
                                     }
                                 }
-                        };
-                        if (n3l) {
-                            const int64_t qo = qoff[cl];
-                            if (qo < 0) update(coef);
-                            else update(a.ion_coef + qo);
                         }
                         /* P_ion of the cell: the sum over its four lanes */
 #pragma unroll
@@ -612,7 +675,7 @@ __global__ void __launch_bounds__(IonPipe<R, NP, S>::THREADS, 1)
                             q1 += __shfl_xor_sync(0xffffffffu, q1, m);
                             q2 += __shfl_xor_sync(0xffffffffu, q2, m);
                         }
-                        if (n3l && tig == 0) {
+                        if (n3l[mt] && tig == 0) {
                             const int64_t sl = x0 + cl;
                             a.pr[sl] = q0;
                             a.pr[ns + sl] = q1;
