@@ -531,6 +531,7 @@ def run_serving(args, ws, rank, local):
     bad = [i for i in infos.values() if i["status"] != 0]
     lat = np.array([infos[q]["t_done"] - infos[q]["t_submit"] for q in range(len(reqs))])
     queue_wait = np.array([infos[q]["t_admit"] - infos[q]["t_submit"] for q in range(len(reqs))])
+    build = np.array([infos[q]["t_start"] - infos[q]["t_admit"] for q in range(len(reqs))])
     t_first = min(i["t_submit"] for i in infos.values())
     t_last = max(i["t_done"] for i in infos.values())
     makespan = t_last - t_first
@@ -570,7 +571,9 @@ def run_serving(args, ws, rank, local):
                    "memory_budget_bytes": budget, "max_active": args.max_active, "chunk_steps": 256},
         "latency_s": {"p50": round(float(np.percentile(lat, 50)), 3), "p95": round(float(np.percentile(lat, 95)), 3),
                       "p99": round(float(np.percentile(lat, 99)), 3), "max": round(float(lat.max()), 3),
-                      "queue_wait_p50": round(float(np.percentile(queue_wait, 50)), 3)},
+                      "queue_wait_p50": round(float(np.percentile(queue_wait, 50)), 3),
+                      "build_p50": round(float(np.percentile(build, 50)), 4),
+                      "build_p99": round(float(np.percentile(build, 99)), 4)},
         "makespan_s": round(makespan, 3), "gcell_updates_per_s": round(float(cs.sum()) / makespan / 1e9, 3),
         "failed": len(bad), "server": stats,
         "baseline_sequential_fp64": {"sims_per_h": round(seq_sims_h, 2), "sample": len(sample),

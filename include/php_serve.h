@@ -60,6 +60,7 @@ typedef struct {
     int32_t status;            /* PHP_OK or the PHP_ERR_* code of the failing call */
     int32_t steps;             /* time steps run */
     double t_submit, t_admit, t_done;
+    double t_start;            /* context built, first chunk about to be queued */
     uint64_t device_bytes;     /* footprint charged against the budget */
     int32_t nx, ny, nfreq;     /* shape of the DFT result */
     int32_t dft_samples;

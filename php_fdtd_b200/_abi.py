@@ -81,7 +81,7 @@ class DftRequest(C.Structure):
 
 class JobInfo(C.Structure):
     _fields_ = [("job", C.c_int64), ("tag", C.c_uint64), ("status", _i), ("steps", _i), ("t_submit", _d),
-                ("t_admit", _d), ("t_done", _d), ("device_bytes", C.c_uint64), ("nx", _i), ("ny", _i), ("nfreq", _i),
+                ("t_admit", _d), ("t_done", _d), ("t_start", _d), ("device_bytes", C.c_uint64), ("nx", _i), ("ny", _i), ("nfreq", _i),
                 ("dft_samples", _i), ("error", C.c_char * 256)]
 
 

@@ -54,7 +54,7 @@ def _run(cmd, verbose):
 
 def build_host(verbose: bool = False) -> Path:
     out = PKG / "libphphost.so"
-    deps = [HOST / "php_host.c", INC / "php_host.h", INC / "php_fdtd.h"]
+    deps = [HOST / "php_host.c", INC / "php_host.h", INC / "php_fdtd.h", INC / "php_serve.h"]
     if _stale(out, deps):
         _run([_cc(), "-O2", "-ffp-contract=off", "-fno-fast-math", "-std=gnu11", "-fPIC", "-shared",
               "-Wall", "-Wextra", "-Wno-unused-parameter", "-Wno-format-truncation", f"-I{INC}", HOST / "php_host.c",
@@ -65,7 +65,7 @@ def build_host(verbose: bool = False) -> Path:
 def build_device(verbose: bool = False) -> Path:
     out = PKG / "libphpfdtd.so"
     sources = [CSRC / "php_fdtd.cu", CSRC / "php_noalloc.cu", CSRC / "php_serve.cu"]
-    deps = sources + [INC / "php_fdtd.h"] + [p for p in CSRC.glob("*.cuh")]
+    deps = sources + [INC / "php_fdtd.h", INC / "php_serve.h"] + [p for p in CSRC.glob("*.cuh")]
     if _stale(out, deps):
         _run([_nvcc(), *NVCC_ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",
               "-shared", f"-I{INC}", *sources, "-o", out], verbose)

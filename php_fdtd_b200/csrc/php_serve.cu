@@ -193,6 +193,7 @@ void admission_loop(php_server* s)
         lk.lock();
         s->building--;
         s->cv_step.notify_one();
+        j->info.t_start = now_since(s->t0);
         if (ok) {
             s->ready.push_back(j);
         } else {

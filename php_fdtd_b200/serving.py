@@ -78,7 +78,7 @@ class Server:
         for k in range(n.value):
             b = buf[k]
             out.append({"job": b.job, "tag": b.tag, "status": b.status, "steps": b.steps, "t_submit": b.t_submit,
-                        "t_admit": b.t_admit, "t_done": b.t_done, "device_bytes": b.device_bytes, "nx": b.nx,
+                        "t_admit": b.t_admit, "t_start": b.t_start, "t_done": b.t_done, "device_bytes": b.device_bytes, "nx": b.nx,
                         "ny": b.ny, "nfreq": b.nfreq, "dft_samples": b.dft_samples,
                         "error": b.error.decode(errors="replace")})
         return out
