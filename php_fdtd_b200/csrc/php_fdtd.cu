@@ -64,6 +64,16 @@ struct php_ctx {
     int num_sms = 148;
     bool any_ade = false, any_atoms = false;
     cudaStream_t stream = nullptr;
+    /* php_create's own work (allocation, zeroing, uploads) runs on a stream
+     * of the highest priority, so that a context built while others keep the
+     * device busy does not queue behind their sweeps; `stream` (default
+     * priority) takes over at the end of php_create */
+    cudaStream_t setup = nullptr;
+    /* page-locked staging of host -> device uploads (upload()) */
+    void* up_buf[2] = {};
+    cudaEvent_t up_ev[2] = {};
+    bool up_used[2] = {};
+    int up_next = 0;
     std::string err;
     uint64_t bytes = 0;
     std::vector<void*> allocs;
@@ -210,6 +220,8 @@ static int dalloc(php_ctx* ctx, void** p, size_t bytes)
     if (e != cudaSuccess) return fail(ctx, PHP_ERR_CUDA, "cudaMemset failed: %s", cudaGetErrorString(e));
     return PHP_OK;
 }
+
+static int upload(php_ctx* ctx, void* dst, const void* src, size_t bytes);
 
 static size_t rsize(int prec) { return prec == PHP_PREC_FP32 ? sizeof(float) : sizeof(double); }
 
@@ -760,12 +772,12 @@ static int upload_tables(php_ctx* ctx, const std::vector<MatD>& mats, const std:
     }
     int rc = dalloc(ctx, &ctx->mc, mc.size() * sizeof(MatCoef<R>));
     if (rc) return rc;
-    CK(cudaMemcpyAsync(ctx->mc, mc.data(), mc.size() * sizeof(MatCoef<R>), cudaMemcpyHostToDevice, ctx->stream));
+    if ((rc = upload(ctx, ctx->mc, mc.data(), mc.size() * sizeof(MatCoef<R>)))) return rc;
     std::vector<R> ic(ion_coef.size() ? ion_coef.size() : 1);
     for (size_t i = 0; i < ion_coef.size(); i++) ic[i] = (R)ion_coef[i];
     rc = dalloc(ctx, &ctx->ion_coef, ic.size() * sizeof(R));
     if (rc) return rc;
-    CK(cudaMemcpyAsync(ctx->ion_coef, ic.data(), ic.size() * sizeof(R), cudaMemcpyHostToDevice, ctx->stream));
+    if ((rc = upload(ctx, ctx->ion_coef, ic.data(), ic.size() * sizeof(R)))) return rc;
     for (int ax = 0; ax < 3; ax++) {
         const AxisD& A = axes[ax];
         const std::vector<double>* cols[7] = {&A.kappa, &A.b, &A.c, &A.kh, &A.kd, &A.ch, &A.cd};
@@ -774,12 +786,11 @@ static int upload_tables(php_ctx* ctx, const std::vector<MatD>& mats, const std:
             for (size_t i = 0; i < h.size(); i++) h[i] = (R)(*cols[q])[i];
             rc = dalloc(ctx, &ctx->axis_tab[ax][q], h.size() * sizeof(R));
             if (rc) return rc;
-            CK(cudaMemcpyAsync(ctx->axis_tab[ax][q], h.data(), h.size() * sizeof(R), cudaMemcpyHostToDevice, ctx->stream));
+            if ((rc = upload(ctx, ctx->axis_tab[ax][q], h.data(), h.size() * sizeof(R)))) return rc;
         }
         rc = dalloc(ctx, (void**)&ctx->axis_slot[ax], A.slot.size() * sizeof(int32_t));
         if (rc) return rc;
-        CK(cudaMemcpyAsync(ctx->axis_slot[ax], A.slot.data(), A.slot.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
-                           ctx->stream));
+        if ((rc = upload(ctx, ctx->axis_slot[ax], A.slot.data(), A.slot.size() * sizeof(int32_t)))) return rc;
     }
     /* host tables must stay alive until the copies finish */
     CK(cudaStreamSynchronize(ctx->stream));
@@ -821,6 +832,49 @@ static void pinned_put(void* p)
     g_pinned_free.emplace(g_pinned_size[p], p);
 }
 
+/* Host -> device copy through page-locked staging.  A copy from pageable
+ * memory is staged by the driver in small synchronous pieces; while other
+ * contexts kept the device busy that took up to seconds per context.  Here
+ * chunks of up to kUploadChunk go through two pooled page-locked buffers,
+ * one copy in flight while the other buffer fills.  The source may be freed
+ * on return. */
+constexpr size_t kUploadChunk = (size_t)4 << 20;
+static int upload(php_ctx* ctx, void* dst, const void* src, size_t bytes)
+{
+    if (bytes == 0) return PHP_OK;
+    for (int b = 0; b < 2; ++b) {
+        if (!ctx->up_buf[b]) {
+            ctx->up_buf[b] = pinned_get(kUploadChunk);
+            if (!ctx->up_buf[b]) return fail(ctx, PHP_ERR_OOM, "page-locked host allocation failed");
+            ctx->up_used[b] = false;
+        }
+        if (!ctx->up_ev[b]) CK(cudaEventCreateWithFlags(&ctx->up_ev[b], cudaEventDisableTiming));
+    }
+    for (size_t off = 0; off < bytes;) {
+        const int b = ctx->up_next & 1;
+        const size_t n = std::min(kUploadChunk, bytes - off);
+        if (ctx->up_used[b]) CK(cudaEventSynchronize(ctx->up_ev[b])); /* its last copy has left */
+        memcpy(ctx->up_buf[b], (const char*)src + off, n);
+        CK(cudaMemcpyAsync((char*)dst + off, ctx->up_buf[b], n, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaEventRecord(ctx->up_ev[b], ctx->stream));
+        ctx->up_used[b] = true;
+        ctx->up_next++;
+        off += n;
+    }
+    return PHP_OK;
+}
+
+/* returns the staging buffers to the pool once their copies are done */
+static void upload_release(php_ctx* ctx)
+{
+    for (int b = 0; b < 2; ++b) {
+        if (ctx->up_used[b]) cudaEventSynchronize(ctx->up_ev[b]);
+        pinned_put(ctx->up_buf[b]);
+        ctx->up_buf[b] = nullptr;
+        ctx->up_used[b] = false;
+    }
+}
+
 static void ctx_free(php_ctx* ctx)
 {
     if (!ctx) return;
@@ -836,6 +890,9 @@ static void ctx_free(php_ctx* ctx)
         pinned_put(ctx->step_in_host[b]);
         if (ctx->staged[b]) cudaEventDestroy(ctx->staged[b]);
     }
+    upload_release(ctx);
+    for (int b = 0; b < 2; ++b)
+        if (ctx->up_ev[b]) cudaEventDestroy(ctx->up_ev[b]);
     for (auto& f : ctx->frames) {
         if (f.done) cudaEventDestroy(f.done);
         pinned_put(f.head);
@@ -843,6 +900,10 @@ static void ctx_free(php_ctx* ctx)
         pinned_put(f.rows);
     }
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->setup && ctx->setup != ctx->stream) {
+        cudaStreamSynchronize(ctx->setup);
+        cudaStreamDestroy(ctx->setup);
+    }
     delete ctx;
 }
 
@@ -926,7 +987,7 @@ static int setup_ion_pass(php_ctx* ctx, const std::vector<MatD>& mats, const std
                 img[(size_t)np * np + off] = lo;
             }
         if ((rc = dalloc(ctx, &ctx->ion_bsplit, img.size() * 2))) return rc;
-        CK(cudaMemcpyAsync(ctx->ion_bsplit, img.data(), img.size() * 2, cudaMemcpyHostToDevice, ctx->stream));
+        if ((rc = upload(ctx, ctx->ion_bsplit, img.data(), img.size() * 2))) return rc;
         CK(cudaStreamSynchronize(ctx->stream));
         ctx->ion_tc = true;
     } else {
@@ -934,7 +995,7 @@ static int setup_ion_pass(php_ctx* ctx, const std::vector<MatD>& mats, const std
         for (int q = 0; q < n3; q++)
             for (int p = 0; p < n3; p++) pad[(size_t)q * np + p] = D[(size_t)q * n3 + p];
         if ((rc = dalloc(ctx, &ctx->ion_dmm, pad.size() * sizeof(double)))) return rc;
-        CK(cudaMemcpyAsync(ctx->ion_dmm, pad.data(), pad.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        if ((rc = upload(ctx, ctx->ion_dmm, pad.data(), pad.size() * sizeof(double)))) return rc;
         /* the same matrix as B fragments of the m8n8k4 FP64 MMA (B[k][n] =
          * DMM[n][k]): lane l of fragment (ks, nt) holds B[4 ks + l % 4][8 nt + l / 4];
          * then the E step, B[t][q] = -QeZM(q, t) (t < 3), and P_ion's B[p][c] =
@@ -960,7 +1021,7 @@ static int setup_ion_pass(php_ctx* ctx, const std::vector<MatD>& mats, const std
                 frag[fp + (size_t)ks * 32 + l] = (c < 3 && p < n3) ? zv[(p / 3) * 9 + c * 3 + p % 3] : 0.0;
             }
         if ((rc = dalloc(ctx, &ctx->ion_dfrag, frag.size() * sizeof(double)))) return rc;
-        CK(cudaMemcpyAsync(ctx->ion_dfrag, frag.data(), frag.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        if ((rc = upload(ctx, ctx->ion_dfrag, frag.data(), frag.size() * sizeof(double)))) return rc;
         CK(cudaStreamSynchronize(ctx->stream));
     }
     ctx->ion_np = np;
@@ -1014,7 +1075,12 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
     if (d.device < 0 || d.device >= ndev) return fail(ctx, PHP_ERR_INPUT, "device %d not present", d.device);
     CK(cudaSetDevice(d.device));
     CK(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, d.device));
-    CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    {
+        int least = 0, greatest = 0;
+        CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        CK(cudaStreamCreateWithPriority(&ctx->setup, cudaStreamNonBlocking, greatest));
+        ctx->stream = ctx->setup;
+    }
 
     /* materials */
     std::vector<MatD> mats(d.num_materials);
@@ -1141,25 +1207,24 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
     }
     int rc = dalloc(ctx, (void**)&ctx->mat, mat_dev.size());
     if (rc) return rc;
-    CK(cudaMemcpyAsync(ctx->mat, mat_dev.data(), mat_dev.size(), cudaMemcpyHostToDevice, ctx->stream));
+    if ((rc = upload(ctx, ctx->mat, mat_dev.data(), mat_dev.size()))) return rc;
     if (ctx->nslot > 0) {
         slot_dev.assign((size_t)ctx->ncell_dev, -1);
         for (int64_t s = 0; s < nreal; s++) slot_dev[slot_cell[s]] = (int32_t)s;
         rc = dalloc(ctx, (void**)&ctx->slot, slot_dev.size() * sizeof(int32_t));
         if (rc) return rc;
-        CK(cudaMemcpyAsync(ctx->slot, slot_dev.data(), slot_dev.size() * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
+        if ((rc = upload(ctx, ctx->slot, slot_dev.data(), slot_dev.size() * sizeof(int32_t)))) return rc;
         rc = dalloc(ctx, (void**)&ctx->slot_cell, slot_cell.size() * sizeof(int64_t));
         if (rc) return rc;
-        CK(cudaMemcpyAsync(ctx->slot_cell, slot_cell.data(), slot_cell.size() * sizeof(int64_t), cudaMemcpyHostToDevice,
-                           ctx->stream));
+        if ((rc = upload(ctx, ctx->slot_cell, slot_cell.data(), slot_cell.size() * sizeof(int64_t)))) return rc;
         rc = dalloc(ctx, (void**)&ctx->slot_n3, slot_n3.size() * sizeof(int32_t));
         if (rc) return rc;
-        CK(cudaMemcpyAsync(ctx->slot_n3, slot_n3.data(), slot_n3.size() * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
+        if ((rc = upload(ctx, ctx->slot_n3, slot_n3.data(), slot_n3.size() * sizeof(int32_t)))) return rc;
         std::vector<uint8_t> slot_mat(slot_cell.size(), 0);
         for (int64_t s = 0; s < nreal; s++) slot_mat[s] = mat_dev[slot_cell[s]];
         rc = dalloc(ctx, (void**)&ctx->slot_mat, slot_mat.size());
         if (rc) return rc;
-        CK(cudaMemcpyAsync(ctx->slot_mat, slot_mat.data(), slot_mat.size(), cudaMemcpyHostToDevice, ctx->stream));
+        if ((rc = upload(ctx, ctx->slot_mat, slot_mat.data(), slot_mat.size()))) return rc;
         CK(cudaStreamSynchronize(ctx->stream)); /* the host vectors go out of scope */
     }
     if (ctx->any_ade) {
@@ -1206,6 +1271,13 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
     ctx->host_stage = pinned_get(ctx->host_stage_bytes);
     if (!ctx->host_stage) return fail(ctx, PHP_ERR_OOM, "page-locked host allocation failed");
     CK(cudaStreamSynchronize(ctx->stream));
+    upload_release(ctx);
+    /* hand over to the context's stream (everything above is complete) */
+    cudaStream_t work = nullptr;
+    CK(cudaStreamCreateWithFlags(&work, cudaStreamNonBlocking));
+    ctx->stream = work;
+    cudaStreamDestroy(ctx->setup);
+    ctx->setup = nullptr;
     return PHP_OK;
 }
 
