@@ -74,7 +74,10 @@ struct php_ctx {
     cudaEvent_t up_ev[2] = {};
     bool up_used[2] = {};
     int up_next = 0;
-    std::string err;
+    /* last error text: a fixed buffer, so that php_last_error's pointer stays
+     * valid while another thread (php_frame_wait) records an error */
+    char err[1024] = "";
+    std::mutex err_mu;
     uint64_t bytes = 0;
     std::vector<void*> allocs;
 
@@ -187,8 +190,12 @@ static int fail(php_ctx* c, int code, const char* fmt, ...)
     va_start(ap, fmt);
     vsnprintf(buf, sizeof(buf), fmt, ap);
     va_end(ap);
-    if (c) c->err = buf;
-    else g_create_error = buf;
+    if (c) {
+        std::lock_guard<std::mutex> g(c->err_mu);
+        memcpy(c->err, buf, sizeof(buf));
+    } else {
+        g_create_error = buf;
+    }
     return code;
 }
 
@@ -1555,7 +1562,7 @@ int php_destroy(php_ctx* ctx)
 const char* php_last_error(const php_ctx* ctx)
 {
     if (!ctx) return g_create_error.c_str();
-    return ctx->err.c_str();
+    return ctx->err;
 }
 
 int php_step(php_ctx* ctx, int32_t nsteps)
