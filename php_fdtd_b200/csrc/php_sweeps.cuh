@@ -451,8 +451,11 @@ __device__ __forceinline__ void e_update(const StepArgs<R>& a, const MatCoef<R>&
             if constexpr (VREG) {
 #pragma unroll
                 for (int q = 0; q < QN; ++q) {
-                    rold[q] = q < n3 ? a.r[(int64_t)q * ns + slot] : R(0);
-                    vold[q] = q < n3 ? a.v[(int64_t)q * ns + slot] : R(0);
+                    /* 32-bit element offsets: the host keeps few-atom pools
+                     * below 2^32 elements */
+                    const uint32_t o = (uint32_t)q * (uint32_t)ns + (uint32_t)slot;
+                    rold[q] = q < n3 ? a.r[o] : R(0);
+                    vold[q] = q < n3 ? a.v[o] : R(0);
                 }
             }
             auto ion_pr = [&](const auto& C) {
@@ -613,7 +616,7 @@ __device__ __forceinline__ void e_update(const StepArgs<R>& a, const MatCoef<R>&
                     acc = m0 * na + m1 * nb + m2 * nc;
                     for_atoms<QN, VREG>(n3, [&](int p) { acc -= C.dmm(q, p) * rold[p]; });
                 }
-                const int64_t o = (int64_t)q * ns + slot;
+                const int64_t o = VREG ? (int64_t)((uint32_t)q * (uint32_t)ns + (uint32_t)slot) : (int64_t)q * ns + slot;
                 R vq;
                 if constexpr (VREG) vq = vold[q];
                 else vq = a.v[o];
