@@ -958,11 +958,14 @@ static double bf16_value(uint16_t b)
 
 /* Many-atom cells (3N >= 24, one DMM shared by every atom material) get the
  * ion pass of php_ions.cuh in the fast FP64 and FP32 paths; PHP_IONS=fused
- * keeps the update inside the E sweep (for A/B timing). */
+ * keeps the update inside the E sweep and PHP_IONS=pass moves few-atom cells
+ * to the pass too (both for A/B timing). */
 static int setup_ion_pass(php_ctx* ctx, const std::vector<MatD>& mats, const std::vector<int>& ion_off, const php_desc& d)
 {
     const char* iv = getenv("PHP_IONS");
-    if ((iv && !strcmp(iv, "fused")) || ctx->prec == PHP_PREC_FP64_STRICT || ctx->n3max < 24 || ctx->n3max > 64)
+    const bool force = iv && !strcmp(iv, "pass");
+    if ((iv && !strcmp(iv, "fused")) || ctx->prec == PHP_PREC_FP64_STRICT || (ctx->n3max < 24 && !force) ||
+        ctx->n3max == 0 || ctx->n3max > 64)
         return PHP_OK;
     int ref = -1;
     for (int i = 0; i < d.num_materials; i++) {
