@@ -116,6 +116,12 @@ struct StepArgs {
      * first kIsoMats ids, 0 for the others: the fused sweep's common case
      * without a load of the material record */
     R iso[kIsoMats];
+    /* per block of the fused sweep: the material id of a plain block (one
+     * plain isotropic material, no CPML or domain-edge cell, no source), 255
+     * for the others; nullptr = no plain blocks.  kdp: dt / d of the axes
+     * outside the CPML (kappa = 1) */
+    const uint8_t* plain_blk;
+    R kdp[3];
     int64_t nslot;
     int32_t nmat;
     int32_t nx, ny, nz, nxp, L, zchunk;

@@ -381,12 +381,62 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
     if (tid == 0)
         for (int p = k0 - 1; p <= min(k1 - 1, k0 - 1 + G::ES - 1); ++p) issue(p);
 
+    const int ho = (ty + 1) * G::BX + tx + G::HALO; /* own cell in a halo box */
+    const int oo = ty * G::TX + tx;                 /* own cell in an own box */
+
+    /* a plain block (one plain isotropic material, no CPML, edge or source
+     * cell; marked on the host): D += curl H with the kappa = 1 factors and
+     * E = iso D, nothing per cell beyond the stencil (the same arithmetic as
+     * the general path below takes for such cells) */
+    const int pm = (!STRICT && a.plain_blk) ? a.plain_blk[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x]
+                                            : 255;
+    if (pm != 255) {
+        const R iso = a.iso[pm];
+        const R kdx = a.kdp[0], kdy = a.kdp[1], kdz = a.kdp[2];
+        for (int k = k0; k < k1; ++k) {
+            bool ok = true;
+            if (k == k0) ok = mbar_wait(&full[0], 0);
+            ok = ok && mbar_wait(&full[(k - k0 + 1) % G::ES], ((k - k0 + 1) / G::ES) & 1);
+            if (ok) {
+                const unsigned char* bp = stage(k - 1);
+                const unsigned char* bc = stage(k);
+                const R* Hxp = reinterpret_cast<const R*>(bp);
+                const R* Hyp = reinterpret_cast<const R*>(bp + HB);
+                const R* Hx = reinterpret_cast<const R*>(bc);
+                const R* Hy = reinterpret_cast<const R*>(bc + HB);
+                const R* Hz = reinterpret_cast<const R*>(bc + 2 * HB);
+                const R* Ds = reinterpret_cast<const R*>(bc + 3 * HB);
+                const R hx0 = Hx[ho], hy0 = Hy[ho], hz0 = Hz[ho];
+                const R dHzy = hz0 - Hz[ho - G::BX], dHyz = hy0 - Hyp[ho], dHxz = hx0 - Hxp[ho];
+                const R dHzx = hz0 - Hz[ho - 1], dHyx = hy0 - Hy[ho - 1], dHxy = hx0 - Hx[ho - G::BX];
+                const R ux = kdy * dHzy - kdz * dHyz;
+                const R uy = -kdx * dHzx + kdz * dHxz;
+                const R uz = kdx * dHyx - kdy * dHxy;
+                const R dx = Ds[oo] + ux, dy = Ds[OB / sizeof(R) + oo] + uy, dz = Ds[2 * (OB / sizeof(R)) + oo] + uz;
+                const int c = (k * a.ny + j) * a.nxp + i;
+                a.f.dx[c] = dx;
+                a.f.dy[c] = dy;
+                a.f.dz[c] = dz;
+                a.f.ex[c] = iso * dx;
+                a.f.ey[c] = iso * dy;
+                a.f.ez[c] = iso * dz;
+            }
+            if (__syncthreads_or(!ok)) {
+                if (tid == 0) atomicExch(a.err, 1);
+                break;
+            }
+            if (tid == 0 && k - 1 + G::ES <= k1 - 1) {
+                fence_proxy_async_smem();
+                issue(k - 1 + G::ES);
+            }
+        }
+        return;
+    }
+
     const bool active = (i < a.nx) && (j < a.ny);
     const bool interior = (i >= 1 && i < a.nx - 1 && j >= 1 && j < a.ny - 1);
     const int sx = active ? ldg(a.tx.slot + i) : -1;
     const int sy = active ? ldg(a.ty.slot + j) : -1;
-    const int ho = (ty + 1) * G::BX + tx + G::HALO; /* own cell in a halo box */
-    const int oo = ty * G::TX + tx;                 /* own cell in an own box */
 
     for (int k = k0; k < k1; ++k) {
         /* CPML state read before the wait (it does not depend on the stages) */
