@@ -87,6 +87,8 @@ struct php_ctx {
     uint8_t* mat = nullptr;
     uint8_t* plain_blk = nullptr; /* plain blocks of the fused sweep (StepArgs::plain_blk) */
     double kdp[3] = {};
+    uint8_t* plain_h = nullptr;   /* plain blocks of the H sweep (StepArgs::plain_h) */
+    double khp[3] = {};
     int32_t* slot = nullptr;
     int64_t* slot_cell = nullptr;
     uint8_t* slot_mat = nullptr;
@@ -537,6 +539,8 @@ static StepArgs<R> make_args(php_ctx* ctx, int s_local)
     for (size_t q = 0; q < ctx->iso_scale.size() && q < (size_t)kIsoMats; q++) a.iso[q] = (R)ctx->iso_scale[q];
     a.plain_blk = ctx->plain_blk;
     for (int q = 0; q < 3; q++) a.kdp[q] = (R)ctx->kdp[q];
+    a.plain_h = ctx->plain_h;
+    for (int q = 0; q < 3; q++) a.khp[q] = (R)ctx->khp[q];
     a.nslot = ctx->nslot;
 #ifndef PHP_SMEM_MATS
 #define PHP_SMEM_MATS 0
@@ -1278,25 +1282,29 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
         const char* pv = getenv("PHP_PLAIN");
         const int gx = (nx + kBlockX - 1) / kBlockX, gy = (ny + kBlockY - 1) / kBlockY;
         const int gz = (nz + ctx->zchunk - 1) / ctx->zchunk;
-        std::vector<uint8_t> pm((size_t)gx * gy * gz, 255);
+        std::vector<uint8_t> pm((size_t)gx * gy * gz, 255), ph(pm.size(), 0);
         std::vector<char> src_tile(pm.size(), 0);
         for (int s = 0; s < ctx->nsrc_active; s++) {
             const int64_t sc = ctx->src_cell[s];
             const int sk = (int)(sc / ctx->plane), sj = (int)((sc % ctx->plane) / nxp), si = (int)(sc % nxp);
             src_tile[((size_t)(sk / ctx->zchunk) * gy + sj / kBlockY) * gx + si / kBlockX] = 1;
         }
-        size_t nplain = 0;
+        size_t nplain = 0, nplain_h = 0;
         for (int bz = 0; bz < gz && !(pv && !strcmp(pv, "0")) && ctx->prec != PHP_PREC_FP64_STRICT; bz++)
             for (int by = 0; by < gy; by++)
                 for (int bx = 0; bx < gx; bx++) {
                     const int i0 = bx * kBlockX, j0 = by * kBlockY, k0 = bz * ctx->zchunk;
                     const int k1 = std::min(k0 + ctx->zchunk, nz);
                     const size_t b = ((size_t)bz * gy + by) * gx + bx;
-                    if (src_tile[b] || i0 < 1 || i0 + kBlockX > nx - 1 || j0 < 1 || j0 + kBlockY > ny - 1) continue;
-                    bool ok = true;
+                    bool ok = i0 + kBlockX <= nx - 1 && j0 + kBlockY <= ny - 1;
                     for (int i = i0; i < i0 + kBlockX && ok; i++) ok = axes[0].slot[i] < 0;
                     for (int j = j0; j < j0 + kBlockY && ok; j++) ok = axes[1].slot[j] < 0;
                     for (int k = k0; k < k1 && ok; k++) ok = axes[2].slot[k] < 0;
+                    if (ok) { /* the H sweep needs no more */
+                        ph[b] = 1;
+                        nplain_h++;
+                    }
+                    if (!ok || src_tile[b] || i0 < 1 || j0 < 1) continue;
                     const int id = mat_dev[((size_t)k0 * ny + j0) * nxp + i0];
                     ok = ok && id < kIsoMats && id < (int)ctx->iso_scale.size() && ctx->iso_scale[id] != 0.0;
                     for (int k = k0; k < k1 && ok; k++)
@@ -1313,6 +1321,13 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
             if ((rc = dalloc(ctx, (void**)&ctx->plain_blk, pm.size()))) return rc;
             if ((rc = upload(ctx, ctx->plain_blk, pm.data(), pm.size()))) return rc;
         }
+        if (nplain_h) {
+            if ((rc = dalloc(ctx, (void**)&ctx->plain_h, ph.size()))) return rc;
+            if ((rc = upload(ctx, ctx->plain_h, ph.data(), ph.size()))) return rc;
+        }
+        ctx->khp[0] = d.dt / (d.mu0 * d.dx * 1.0);
+        ctx->khp[1] = d.dt / (d.mu0 * d.dy * 1.0);
+        ctx->khp[2] = d.dt / (d.mu0 * d.dz * 1.0);
         ctx->kdp[0] = d.dt / (d.dx * 1.0);
         ctx->kdp[1] = d.dt / (d.dy * 1.0);
         ctx->kdp[2] = d.dt / (d.dz * 1.0);

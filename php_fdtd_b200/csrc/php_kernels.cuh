@@ -122,6 +122,10 @@ struct StepArgs {
      * outside the CPML (kappa = 1) */
     const uint8_t* plain_blk;
     R kdp[3];
+    /* per block of the H sweep: 1 for a tile and z chunk with no CPML cell
+     * and every cell updated (i < nx-1, j < ny-1); kh of kappa = 1 */
+    const uint8_t* plain_h;
+    R khp[3];
     int64_t nslot;
     int32_t nmat;
     int32_t nx, ny, nz, nxp, L, zchunk;

@@ -199,6 +199,47 @@ __global__ void __launch_bounds__(kBlockX * kBlockY) h_sweep_tma(const __grid_co
     if (tid == 0)
         for (int p = k0; p <= min(k1, k0 + G::HS - 1); ++p) issue(p);
 
+    const int eo = ty * G::BX + tx; /* own cell in a halo box */
+    const int ho = ty * G::TX + tx; /* own cell in an own box */
+
+    /* a plain block (no CPML cell, every cell updated; marked on the host):
+     * the stencil with the kappa = 1 factors only, the same arithmetic as the
+     * general path below takes for such cells */
+    if (!STRICT && a.plain_h && a.plain_h[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x]) {
+        const R khx = a.khp[0], khy = a.khp[1], khz = a.khp[2];
+        for (int k = k0; k < k1; ++k) {
+            bool ok = true;
+            if (k == k0) ok = mbar_wait(&full[0], 0);
+            ok = ok && mbar_wait(&full[(k + 1 - k0) % G::HS], ((k + 1 - k0) / G::HS) & 1);
+            if (ok) {
+                const unsigned char* b0 = stage(k);
+                const unsigned char* b1 = stage(k + 1);
+                const R* Ex0 = reinterpret_cast<const R*>(b0);
+                const R* Ey0 = reinterpret_cast<const R*>(b0 + EB);
+                const R* Ez0 = reinterpret_cast<const R*>(b0 + 2 * EB);
+                const R* Ex1 = reinterpret_cast<const R*>(b1);
+                const R* Ey1 = reinterpret_cast<const R*>(b1 + EB);
+                const R* Hs = reinterpret_cast<const R*>(b0 + 3 * EB);
+                const R ex0 = Ex0[eo], ey0 = Ey0[eo], ez0 = Ez0[eo];
+                const R dEyz = Ey1[eo] - ey0, dEzy = Ez0[eo + G::BX] - ez0, dEzx = Ez0[eo + 1] - ez0;
+                const R dExz = Ex1[eo] - ex0, dExy = Ex0[eo + G::BX] - ex0, dEyx = Ey0[eo + 1] - ey0;
+                const int c = (k * a.ny + j) * a.nxp + i;
+                a.f.hx[c] = Hs[ho] + (-khy * dEzy + khz * dEyz);
+                a.f.hy[c] = Hs[HB / sizeof(R) + ho] + (khx * dEzx - khz * dExz);
+                a.f.hz[c] = Hs[2 * (HB / sizeof(R)) + ho] + (-khx * dEyx + khy * dExy);
+            }
+            if (__syncthreads_or(!ok)) {
+                if (tid == 0) atomicExch(a.err, 1);
+                break;
+            }
+            if (tid == 0 && k + G::HS <= k1) {
+                fence_proxy_async_smem();
+                issue(k + G::HS);
+            }
+        }
+        return;
+    }
+
     const bool active = (i < a.nx - 1) && (j < a.ny - 1);
     const int L2 = 2 * a.L;
     const int nxp = a.nxp, ny = a.ny;
@@ -214,8 +255,6 @@ __global__ void __launch_bounds__(kBlockX * kBlockY) h_sweep_tma(const __grid_co
     R* __restrict__ hxg = a.f.hx;
     R* __restrict__ hyg = a.f.hy;
     R* __restrict__ hzg = a.f.hz;
-    const int eo = ty * G::BX + tx; /* own cell in a halo box */
-    const int ho = ty * G::TX + tx; /* own cell in an own box */
 
     for (int k = k0; k < k1; ++k) {
         /* CPML state and per-plane values do not depend on the staged planes:
