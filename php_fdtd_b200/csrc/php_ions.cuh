@@ -349,6 +349,17 @@ __global__ void __launch_bounds__(IonPipe<R, NP, S>::THREADS, 1)
             bulk_commit();
             return true;
         };
+        /* cell offsets of this lane's slots of tile kk (-1 past the pool) */
+        int64_t cells[kIonTile / 32];
+        auto fetch_cells = [&](int kk) {
+            const int64_t xk = (int64_t)((int)blockIdx.x + kk * (int)gridDim.x) * kIonTile;
+#pragma unroll
+            for (int u = 0; u < kIonTile / 32; ++u) {
+                const int64_t sl = xk + lane + 32 * u;
+                cells[u] = sl < a.nslot ? a.slot_cell[sl] : -1;
+            }
+        };
+        if (mine > 0) fetch_cells(0);
         for (int k = 0; k < mine; ++k) {
             const int st = k % S;
             bool ok = true;
@@ -374,13 +385,13 @@ __global__ void __launch_bounds__(IonPipe<R, NP, S>::THREADS, 1)
             }
             /* E^{n+1} of the tile's cells, gathered ahead like the rest of the
              * stage (padding slots repeat the last cell; slots past the pool
-             * are not read) */
+             * are not read); their cell offsets were read one tile ahead */
             R* es = reinterpret_cast<R*>(b + P::E_OFF);
 #pragma unroll
             for (int u = 0; u < kIonTile / 32; ++u) {
                 const int t = lane + 32 * u;
-                if ((int64_t)x + t < a.nslot) {
-                    const int64_t c = a.slot_cell[x + t];
+                const int64_t c = cells[u];
+                if (c >= 0) {
                     cp_async_ca<sizeof(R)>(es + t, a.ex + c);
                     cp_async_ca<sizeof(R)>(es + kIonTile + t, a.ey + c);
                     cp_async_ca<sizeof(R)>(es + 2 * kIonTile + t, a.ez + c);
@@ -388,6 +399,7 @@ __global__ void __launch_bounds__(IonPipe<R, NP, S>::THREADS, 1)
             }
             cp_async_arrive_noinc(&full[st]);
             issued = k + 1;
+            if (k + 1 < mine) fetch_cells(k + 1);
         }
         if (lane == 0 && !failed)
             for (int kk = max(0, mine - S); kk < mine && !failed; ++kk) failed = !store_tile(kk);
