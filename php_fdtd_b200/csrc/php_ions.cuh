@@ -605,26 +605,34 @@ __global__ void __launch_bounds__(IonPipe<R, NP, S>::THREADS, 1)
                             dmma_8x8x4(acc[0][nt][0], acc[0][nt][1], a0, b);
                             dmma_8x8x4(acc[1][nt][0], acc[1][nt][1], a1, b);
                         }
-                        /* acc = DMM . r - QeZM . E = -a */
+                        /* acc = DMM . r - QeZM . E = -a.  The update goes cell-major:
+                         * lane l takes cell cb + l % 16 and, per step, the coordinate
+                         * q of columns 2t + j with t = t2 + 2 (l / 16), shuffled in
+                         * from the lane that holds it, so that each shared-memory
+                         * access covers 16 consecutive cells of two rows (no bank
+                         * conflicts; the accumulator layout would give four rows) */
+                        const int me = lane & 15, half = lane >> 4;
+                        const int cme = cb + me;
+                        const bool live_me = x0 + cme < ns && n3s[cme] != 0;
 #pragma unroll
-                        for (int mt = 0; mt < 2; ++mt) {
-                            const int cl = cb + 8 * mt + grp;
-                            if (n3l[mt]) {
+                        for (int nt = 0; nt < NP / 8; ++nt)
 #pragma unroll
-                                for (int nt = 0; nt < NP / 8; ++nt)
+                            for (int j = 0; j < 2; ++j)
 #pragma unroll
-                                    for (int j = 0; j < 2; ++j) {
-                                        const int q = nt * 8 + 2 * tig + j;
-                                        if (q < n3) {
-                                            const R acc_q = -(R)acc[mt][nt][j];
-                                            const int o = q * kIonTile + cl;
-                                            const R vq = vs[o];
-                                            rs[o] = rs[o] + (vq * dt + R(0.5) * acc_q * dt * dt);
-                                            vs[o] = vq + acc_q * dt;
-                                        }
+                                for (int t2 = 0; t2 < 2; ++t2) {
+                                    const int t = t2 + 2 * half;
+                                    const int src = (me & 7) * 4 + t;
+                                    const double v0 = __shfl_sync(0xffffffffu, acc[0][nt][j], src);
+                                    const double v1 = __shfl_sync(0xffffffffu, acc[1][nt][j], src);
+                                    const int q = nt * 8 + 2 * t + j;
+                                    if (live_me && q < n3) {
+                                        const R acc_q = -(R)(me < 8 ? v0 : v1);
+                                        const int o = q * kIonTile + cme;
+                                        const R vq = vs[o];
+                                        rs[o] = rs[o] + (vq * dt + R(0.5) * acc_q * dt * dt);
+                                        vs[o] = vq + acc_q * dt;
                                     }
-                            }
-                        }
+                                }
                         __syncwarp();
                         /* P_ion = QeZV . r^{n+1}: lanes t = 0, 1 of each cell hold
                          * components 2t, 2t + 1 */
