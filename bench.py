@@ -483,8 +483,8 @@ def metric_name(args):
 
 
 def workload_name(args):
-    from php_fdtd_b200.workloads import BASELINE_NAMES
-    return BASELINE_NAMES[WORKLOADS[args.workload]] + ("" if args.scale == 1.0 else f" (scale {args.scale})")
+    from php_fdtd_b200.workloads import CONFIG_NAMES
+    return CONFIG_NAMES[WORKLOADS[args.workload]] + ("" if args.scale == 1.0 else f" (scale {args.scale})")
 
 
 def run_serving(args, ws, rank, local):

@@ -344,7 +344,7 @@ def drude_lorentz_eps(nu_cm: float) -> complex:
     return e
 
 
-BASELINE_NAMES = ["cfg0_polar_slab_96", "cfg1_tip_ade_256", "cfg2_lattice16_512x512x256", "cfg3_serving_request",
+CONFIG_NAMES = ["cfg0_polar_slab_96", "cfg1_tip_ade_256", "cfg2_lattice16_512x512x256", "cfg3_serving_request",
                   "cfg4_largest_1024x1024x512"]
 
 

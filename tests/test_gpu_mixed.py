@@ -1,5 +1,5 @@
 """The FP32 (mixed) path against the FP64 path on a metal-tip case: the
-north-star error bounds (1e-4 relative L2 on the fields, 1e-3 on the
+required error bounds (1e-4 relative L2 on the fields, 1e-3 on the
 running-DFT near-field plane) and the read-back of the ADE state, which the
 FP32 path keeps in increment form."""
 import math

@@ -2,7 +2,7 @@
 
   fp64-strict  bit-identical to the reference (golden fixtures and the drop-in
                executable's files byte for byte)
-  fp64         relative L2 <= 1e-10 on every output (north_star bound)
+  fp64         relative L2 <= 1e-10 on every output (the plain-path bound)
   fp32         relative L2 <= 5e-4 on slices with signal (mixed precision)
 """
 import filecmp
