@@ -1296,26 +1296,29 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
                     const int i0 = bx * kBlockX, j0 = by * kBlockY, k0 = bz * ctx->zchunk;
                     const int k1 = std::min(k0 + ctx->zchunk, nz);
                     const size_t b = ((size_t)bz * gy + by) * gx + bx;
-                    bool ok = i0 + kBlockX <= nx - 1 && j0 + kBlockY <= ny - 1;
-                    for (int i = i0; i < i0 + kBlockX && ok; i++) ok = axes[0].slot[i] < 0;
-                    for (int j = j0; j < j0 + kBlockY && ok; j++) ok = axes[1].slot[j] < 0;
-                    for (int k = k0; k < k1 && ok; k++) ok = axes[2].slot[k] < 0;
-                    if (ok) { /* the H sweep needs no more */
+                    const int i1 = std::min(i0 + kBlockX, nx), j1 = std::min(j0 + kBlockY, ny);
+                    bool pml_free = true;
+                    for (int i = i0; i < i1 && pml_free; i++) pml_free = axes[0].slot[i] < 0;
+                    for (int j = j0; j < j1 && pml_free; j++) pml_free = axes[1].slot[j] < 0;
+                    for (int k = k0; k < k1 && pml_free; k++) pml_free = axes[2].slot[k] < 0;
+                    const bool full = i0 + kBlockX <= nx - 1 && j0 + kBlockY <= ny - 1; /* every cell has i < nx-1, j < ny-1 */
+                    if (full && pml_free) { /* the H sweep needs no more */
                         ph[b] = 1;
                         nplain_h++;
                     }
-                    if (!ok || src_tile[b] || i0 < 1 || j0 < 1) continue;
+                    if (src_tile[b]) continue;
                     const int id = mat_dev[((size_t)k0 * ny + j0) * nxp + i0];
-                    ok = ok && id < kIsoMats && id < (int)ctx->iso_scale.size() && ctx->iso_scale[id] != 0.0;
+                    bool ok = id < kIsoMats && id < (int)ctx->iso_scale.size() && ctx->iso_scale[id] != 0.0;
                     for (int k = k0; k < k1 && ok; k++)
-                        for (int j = j0; j < j0 + kBlockY && ok; j++) {
-                            const uint8_t* row = &mat_dev[((size_t)k * ny + j) * nxp + i0];
-                            for (int i = 0; i < kBlockX && ok; i++) ok = row[i] == id;
+                        for (int j = j0; j < j1 && ok; j++) {
+                            const uint8_t* row = &mat_dev[((size_t)k * ny + j) * nxp];
+                            for (int i = i0; i < i1 && ok; i++) ok = row[i] == id;
                         }
-                    if (ok) {
-                        pm[b] = (uint8_t)id;
-                        nplain++;
-                    }
+                    if (!ok) continue;
+                    /* one plain material: the stencil-only path, or with CPML or
+                     * domain-edge cells the path that adds their CPML terms */
+                    pm[b] = (uint8_t)((full && i0 >= 1 && j0 >= 1 && pml_free) ? id : kPlainCpml + id);
+                    nplain++;
                 }
         if (nplain) {
             if ((rc = dalloc(ctx, (void**)&ctx->plain_blk, pm.size()))) return rc;

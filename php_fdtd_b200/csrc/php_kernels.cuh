@@ -98,6 +98,9 @@ constexpr int kIonKM = 36;
 constexpr int kIonKD = 72;
 constexpr int kIonK = kIonKD + kIonKQ * kIonKQ;
 constexpr int kIsoMats = 32;
+/* plain-block codes of the fused sweep: id, or kPlainCpml + id for blocks of
+ * one plain material with CPML or domain-edge cells; 255 = general path */
+constexpr int kPlainCpml = 64;
 
 template <typename R>
 struct StepArgs {
