@@ -17,6 +17,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -164,6 +165,10 @@ struct php_ctx {
     int ion_k_off = -1;
     std::vector<double> ion_k;
     std::vector<double> iso_scale;   /* StepArgs::iso, per material */
+    /* per material: eps_inv, eps_im, cs, sn of the packed record; the
+     * chosen one rides in StepArgs::tns_* */
+    std::vector<std::array<double, 20>> mat_tns;
+    int tns_id = -1;
 
     /* output frames (php_frame_begin): page-locked slots taken in ticket
      * order; state 0 free, 1 taken (begun and not released) */
@@ -541,6 +546,19 @@ static StepArgs<R> make_args(php_ctx* ctx, int s_local)
     for (int q = 0; q < 3; q++) a.kdp[q] = (R)ctx->kdp[q];
     a.plain_h = ctx->plain_h;
     for (int q = 0; q < 3; q++) a.khp[q] = (R)ctx->khp[q];
+    a.tns_flags = 0;
+    a.tns_cs = a.tns_sn = R(0);
+    for (int q = 0; q < 9; q++) a.tns_inv[q] = a.tns_im[q] = R(0);
+    if (ctx->tns_id >= 0) {
+        const std::array<double, 20>& t = ctx->mat_tns[ctx->tns_id];
+        a.tns_flags = ctx->mat_flags[ctx->tns_id];
+        for (int q = 0; q < 9; q++) {
+            a.tns_inv[q] = (R)t[q];
+            a.tns_im[q] = (R)t[9 + q];
+        }
+        a.tns_cs = (R)t[18];
+        a.tns_sn = (R)t[19];
+    }
     a.nslot = ctx->nslot;
 #ifndef PHP_SMEM_MATS
 #define PHP_SMEM_MATS 0
@@ -781,9 +799,16 @@ static int upload_tables(php_ctx* ctx, const std::vector<MatD>& mats, const std:
 {
     std::vector<MatCoef<R>> mc(mats.size());
     ctx->iso_scale.assign(mats.size(), 0.0);
+    ctx->mat_tns.assign(mats.size(), {});
     for (size_t i = 0; i < mats.size(); i++) {
         mc[i] = pack_material<R>(ctx, mats[i], ion_off[i]);
         if (mc[i].flags & kIso) ctx->iso_scale[i] = (double)mc[i].eps_inv[0];
+        for (int q = 0; q < 9; q++) {
+            ctx->mat_tns[i][q] = (double)mc[i].eps_inv[q];
+            ctx->mat_tns[i][9 + q] = (double)mc[i].eps_im[q];
+        }
+        ctx->mat_tns[i][18] = (double)mc[i].cs;
+        ctx->mat_tns[i][19] = (double)mc[i].sn;
     }
     int rc = dalloc(ctx, &ctx->mc, mc.size() * sizeof(MatCoef<R>));
     if (rc) return rc;
@@ -1277,7 +1302,10 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
      * one plain isotropic material (id < kIsoMats), none in the CPML, none
      * on the domain's x/y edge, no source.  The sweep updates them without
      * the per-cell material, CPML and source handling; PHP_PLAIN=0 turns it
-     * off (A/B timing and tests). */
+     * off (A/B timing and tests).  Blocks without a source of the one lossy
+     * or anisotropic material (no ADE, no ions) that fills the most blocks
+     * take its coefficients from the kernel parameters (kPlainTensor;
+     * PHP_PLAIN_TENSOR=0 turns that class off). */
     {
         const char* pv = getenv("PHP_PLAIN");
         const int gx = (nx + kBlockX - 1) / kBlockX, gy = (ny + kBlockY - 1) / kBlockY;
@@ -1290,6 +1318,10 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
             src_tile[((size_t)(sk / ctx->zchunk) * gy + sj / kBlockY) * gx + si / kBlockX] = 1;
         }
         size_t nplain = 0, nplain_h = 0;
+        const char* tv = getenv("PHP_PLAIN_TENSOR");
+        const bool tns_off = tv && !strcmp(tv, "0");
+        std::vector<int16_t> uni(pm.size(), -1);
+        std::vector<size_t> tns_count(ctx->mat_flags.size(), 0);
         for (int bz = 0; bz < gz && !(pv && !strcmp(pv, "0")) && ctx->prec != PHP_PREC_FP64_STRICT; bz++)
             for (int by = 0; by < gy; by++)
                 for (int bx = 0; bx < gx; bx++) {
@@ -1308,16 +1340,30 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
                     }
                     if (src_tile[b]) continue;
                     const int id = mat_dev[((size_t)k0 * ny + j0) * nxp + i0];
-                    bool ok = id < kIsoMats && id < (int)ctx->iso_scale.size() && ctx->iso_scale[id] != 0.0;
+                    bool ok = id < (int)ctx->mat_flags.size() && id < (int)ctx->iso_scale.size();
                     for (int k = k0; k < k1 && ok; k++)
                         for (int j = j0; j < j1 && ok; j++) {
                             const uint8_t* row = &mat_dev[((size_t)k * ny + j) * nxp];
                             for (int i = i0; i < i1 && ok; i++) ok = row[i] == id;
                         }
                     if (!ok) continue;
-                    /* one plain material: the stencil-only path, or with CPML or
-                     * domain-edge cells the path that adds their CPML terms */
-                    pm[b] = (uint8_t)((full && i0 >= 1 && j0 >= 1 && pml_free) ? id : kPlainCpml + id);
+                    if (id < kIsoMats && ctx->iso_scale[id] != 0.0) {
+                        /* one plain material: the stencil-only path, or with CPML or
+                         * domain-edge cells the path that adds their CPML terms */
+                        pm[b] = (uint8_t)((full && i0 >= 1 && j0 >= 1 && pml_free) ? id : kPlainCpml + id);
+                        nplain++;
+                    } else if (!(ctx->mat_flags[id] & (kAde | kAtoms)) && ctx->iso_scale[id] == 0.0 && !tns_off) {
+                        uni[b] = (int16_t)id; /* a tensor block if id is the material chosen below */
+                        tns_count[id]++;
+                    }
+                }
+        /* the lossy or anisotropic material filling the most blocks */
+        for (size_t id = 0; id < tns_count.size(); id++)
+            if (tns_count[id] && (ctx->tns_id < 0 || tns_count[id] > tns_count[ctx->tns_id])) ctx->tns_id = (int)id;
+        if (ctx->tns_id >= 0)
+            for (size_t b = 0; b < pm.size(); b++)
+                if (uni[b] == ctx->tns_id) {
+                    pm[b] = (uint8_t)kPlainTensor;
                     nplain++;
                 }
         if (nplain) {

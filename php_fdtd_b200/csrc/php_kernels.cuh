@@ -99,8 +99,10 @@ constexpr int kIonKD = 72;
 constexpr int kIonK = kIonKD + kIonKQ * kIonKQ;
 constexpr int kIsoMats = 32;
 /* plain-block codes of the fused sweep: id, or kPlainCpml + id for blocks of
- * one plain material with CPML or domain-edge cells; 255 = general path */
+ * one plain material with CPML or domain-edge cells, kPlainTensor for blocks
+ * of the tensor material in StepArgs::tns_*; 255 = general path */
 constexpr int kPlainCpml = 64;
+constexpr int kPlainTensor = 128;
 
 template <typename R>
 struct StepArgs {
@@ -129,6 +131,11 @@ struct StepArgs {
      * and every cell updated (i < nx-1, j < ny-1); kh of kappa = 1 */
     const uint8_t* plain_h;
     R khp[3];
+    /* the material record of one lossy or anisotropic material without ADE
+     * or ions (the one filling most blocks): blocks of that material alone
+     * (kPlainTensor) read it as constant-bank operands */
+    R tns_inv[9], tns_im[9], tns_cs, tns_sn;
+    int32_t tns_flags;
     int64_t nslot;
     int32_t nmat;
     int32_t nx, ny, nz, nxp, L, zchunk;

@@ -429,6 +429,88 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
      * the general path below takes for such cells) */
     const int pm = (!STRICT && a.plain_blk) ? a.plain_blk[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x]
                                             : 255;
+    if (pm == kPlainTensor) {
+        /* one lossy or anisotropic material (no ADE, ions or source): the
+         * general path's D update with the eps'' term and E = eps^-1 D in
+         * the crystal frame, its coefficients from the kernel parameters and
+         * the old E read before the stage wait (it does not depend on the
+         * stages) */
+        const bool active = (i < a.nx) && (j < a.ny);
+        const bool interior = (i >= 1 && i < a.nx - 1 && j >= 1 && j < a.ny - 1);
+        const int sx = active ? ldg(a.tx.slot + i) : -1;
+        const int sy = active ? ldg(a.ty.slot + j) : -1;
+        const int fl = a.tns_flags;
+        const bool lossy = (fl & kLossy) != 0;
+        constexpr bool kInc = sizeof(R) == 4;
+        for (int k = k0; k < k1; ++k) {
+            CellPsi<R> ps;
+            ps.sz = -1;
+            if (active && interior) load_psi_d(a, i, j, k, sx, sy, ps);
+            const int c = (k * a.ny + j) * a.nxp + i;
+            R ex = R(0), ey = R(0), ez = R(0);
+            if (active && interior && lossy) {
+                ex = a.f.ex[c];
+                ey = a.f.ey[c];
+                ez = a.f.ez[c];
+            }
+            bool ok = true;
+            if (k == k0) ok = mbar_wait(&full[0], 0);
+            ok = ok && mbar_wait(&full[(k - k0 + 1) % G::ES], ((k - k0 + 1) / G::ES) & 1);
+            if (ok && active) {
+                const unsigned char* bp = stage(k - 1);
+                const unsigned char* bc = stage(k);
+                const R* Hxp = reinterpret_cast<const R*>(bp);
+                const R* Hyp = reinterpret_cast<const R*>(bp + HB);
+                const R* Hx = reinterpret_cast<const R*>(bc);
+                const R* Hy = reinterpret_cast<const R*>(bc + HB);
+                const R* Hz = reinterpret_cast<const R*>(bc + 2 * HB);
+                const R* Ds = reinterpret_cast<const R*>(bc + 3 * HB);
+                R dx = Ds[oo], dy = Ds[OB / sizeof(R) + oo], dz = Ds[2 * (OB / sizeof(R)) + oo];
+                R ix = R(0), iy = R(0), iz = R(0);
+                R& ux = kInc ? ix : dx;
+                R& uy = kInc ? iy : dy;
+                R& uz = kInc ? iz : dz;
+                if (interior) {
+                    d_update<R, false>(a, i, j, k, sx, sy, Hx[ho], Hy[ho], Hz[ho], Hxp[ho], Hyp[ho], Hz[ho - G::BX],
+                                       Hx[ho - G::BX], Hz[ho - 1], Hy[ho - 1], ps, ux, uy, uz);
+                    if (lossy) { /* fdtd.c:3349-3353 */
+                        const R* q = a.tns_im;
+                        ux -= q[0] * ex + q[1] * ey + q[2] * ez;
+                        uy -= q[3] * ex + q[4] * ey + q[5] * ez;
+                        uz -= q[6] * ex + q[7] * ey + q[8] * ez;
+                    }
+                }
+                if constexpr (kInc) {
+                    dx += ix;
+                    dy += iy;
+                    dz += iz;
+                }
+                /* fdtd.c:3429-3461, 3486-3503 */
+                R da = dx, db = dy, dc = dz;
+                rot_fwd<false>(fl, a.tns_cs, a.tns_sn, da, db, dc);
+                const R* E = a.tns_inv;
+                R na = E[0] * da + E[1] * db + E[2] * dc;
+                R nb = E[3] * da + E[4] * db + E[5] * dc;
+                R nc = E[6] * da + E[7] * db + E[8] * dc;
+                rot_back<false>(fl, a.tns_cs, a.tns_sn, na, nb, nc);
+                a.f.dx[c] = dx;
+                a.f.dy[c] = dy;
+                a.f.dz[c] = dz;
+                a.f.ex[c] = na;
+                a.f.ey[c] = nb;
+                a.f.ez[c] = nc;
+            }
+            if (__syncthreads_or(!ok)) {
+                if (tid == 0) atomicExch(a.err, 1);
+                break;
+            }
+            if (tid == 0 && k - 1 + G::ES <= k1 - 1) {
+                fence_proxy_async_smem();
+                issue(k - 1 + G::ES);
+            }
+        }
+        return;
+    }
     if (pm != 255 && pm >= kPlainCpml) {
         /* one plain material with CPML or domain-edge cells: the general
          * path's D update (CPML terms included) and E = iso D, without the
