@@ -169,6 +169,11 @@ struct php_ctx {
      * chosen one rides in StepArgs::tns_* */
     std::vector<std::array<double, 20>> mat_tns;
     int tns_id = -1;
+    /* the few-atom material of ion_k and its packed record (MatCoef<R>
+     * bytes), for StepArgs::amc; atom_blocks: kPlainAtoms blocks exist */
+    int atom_id = -1;
+    std::vector<unsigned char> atom_mc;
+    bool atom_blocks = false;
 
     /* output frames (php_frame_begin): page-locked slots taken in ticket
      * order; state 0 free, 1 taken (begun and not released) */
@@ -559,6 +564,8 @@ static StepArgs<R> make_args(php_ctx* ctx, int s_local)
         a.tns_cs = (R)t[18];
         a.tns_sn = (R)t[19];
     }
+    memset(&a.amc, 0, sizeof(a.amc));
+    if (ctx->atom_blocks && ctx->atom_mc.size() == sizeof(MatCoef<R>)) memcpy(&a.amc, ctx->atom_mc.data(), sizeof(MatCoef<R>));
     a.nslot = ctx->nslot;
 #ifndef PHP_SMEM_MATS
 #define PHP_SMEM_MATS 0
@@ -809,6 +816,10 @@ static int upload_tables(php_ctx* ctx, const std::vector<MatD>& mats, const std:
         }
         ctx->mat_tns[i][18] = (double)mc[i].cs;
         ctx->mat_tns[i][19] = (double)mc[i].sn;
+        if ((int)i == ctx->atom_id) {
+            const unsigned char* p = reinterpret_cast<const unsigned char*>(&mc[i]);
+            ctx->atom_mc.assign(p, p + sizeof(MatCoef<R>));
+        }
     }
     int rc = dalloc(ctx, &ctx->mc, mc.size() * sizeof(MatCoef<R>));
     if (rc) return rc;
@@ -1197,6 +1208,7 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
             for (int q = 0; q < n3; q++)
                 for (int p = 0; p < n3; p++) ctx->ion_k[kIonKD + q * kIonKQ + p] = M.dmm[(size_t)q * n3 + p];
             ctx->ion_k_off = ion_off[best];
+            ctx->atom_id = best;
         }
     }
     const int namax = n3max / 3;
@@ -1305,7 +1317,9 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
      * off (A/B timing and tests).  Blocks without a source of the one lossy
      * or anisotropic material (no ADE, no ions) that fills the most blocks
      * take its coefficients from the kernel parameters (kPlainTensor;
-     * PHP_PLAIN_TENSOR=0 turns that class off). */
+     * PHP_PLAIN_TENSOR=0 turns that class off), and so do blocks of the
+     * few-atom material whose ions the sweep updates (kPlainAtoms;
+     * PHP_PLAIN_ATOMS=0). */
     {
         const char* pv = getenv("PHP_PLAIN");
         const int gx = (nx + kBlockX - 1) / kBlockX, gy = (ny + kBlockY - 1) / kBlockY;
@@ -1320,6 +1334,12 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
         size_t nplain = 0, nplain_h = 0;
         const char* tv = getenv("PHP_PLAIN_TENSOR");
         const bool tns_off = tv && !strcmp(tv, "0");
+        /* blocks of the few-atom material when the fused sweep updates its
+         * ions (two or four atoms, no ion pass apart) */
+        const char* av = getenv("PHP_PLAIN_ATOMS");
+        const bool atoms_on = !(av && !strcmp(av, "0")) && ctx->atom_id >= 0 && !ctx->ion_split &&
+                              (ctx->namax_tpl == 2 || ctx->namax_tpl == 4) &&
+                              !(ctx->mat_flags[ctx->atom_id] & kAde) && ctx->atom_mc.size() > 0;
         std::vector<int16_t> uni(pm.size(), -1);
         std::vector<size_t> tns_count(ctx->mat_flags.size(), 0);
         for (int bz = 0; bz < gz && !(pv && !strcmp(pv, "0")) && ctx->prec != PHP_PREC_FP64_STRICT; bz++)
@@ -1352,6 +1372,10 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
                          * domain-edge cells the path that adds their CPML terms */
                         pm[b] = (uint8_t)((full && i0 >= 1 && j0 >= 1 && pml_free) ? id : kPlainCpml + id);
                         nplain++;
+                    } else if (atoms_on && id == ctx->atom_id) {
+                        pm[b] = (uint8_t)kPlainAtoms;
+                        nplain++;
+                        ctx->atom_blocks = true;
                     } else if (!(ctx->mat_flags[id] & (kAde | kAtoms)) && ctx->iso_scale[id] == 0.0 && !tns_off) {
                         uni[b] = (int16_t)id; /* a tensor block if id is the material chosen below */
                         tns_count[id]++;

@@ -100,9 +100,11 @@ constexpr int kIonK = kIonKD + kIonKQ * kIonKQ;
 constexpr int kIsoMats = 32;
 /* plain-block codes of the fused sweep: id, or kPlainCpml + id for blocks of
  * one plain material with CPML or domain-edge cells, kPlainTensor for blocks
- * of the tensor material in StepArgs::tns_*; 255 = general path */
+ * of the tensor material in StepArgs::tns_*, kPlainAtoms for blocks of the
+ * few-atom material in StepArgs::amc; 255 = general path */
 constexpr int kPlainCpml = 64;
 constexpr int kPlainTensor = 128;
+constexpr int kPlainAtoms = 129;
 
 template <typename R>
 struct StepArgs {
@@ -136,6 +138,9 @@ struct StepArgs {
      * (kPlainTensor) read it as constant-bank operands */
     R tns_inv[9], tns_im[9], tns_cs, tns_sn;
     int32_t tns_flags;
+    /* the material record of the few-atom material whose ion coefficients
+     * are in ion_k, for blocks of that material alone (kPlainAtoms) */
+    MatCoef<R> amc;
     int64_t nslot;
     int32_t nmat;
     int32_t nx, ny, nz, nxp, L, zchunk;

@@ -429,6 +429,82 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
      * the general path below takes for such cells) */
     const int pm = (!STRICT && a.plain_blk) ? a.plain_blk[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x]
                                             : 255;
+    if constexpr (NAMAX > 0 && NAMAX <= 4) {
+        if (pm == kPlainAtoms) {
+            /* the few-atom material alone (no ADE, no source): the general
+             * path's D update and D -> E with the fused ion update, its
+             * material record and ion coefficients from the kernel
+             * parameters */
+            const MatCoef<R>& m = a.amc;
+            const bool active = (i < a.nx) && (j < a.ny);
+            const bool interior = (i >= 1 && i < a.nx - 1 && j >= 1 && j < a.ny - 1);
+            const int sx = active ? ldg(a.tx.slot + i) : -1;
+            const int sy = active ? ldg(a.ty.slot + j) : -1;
+            const bool lossy = (m.flags & kLossy) != 0;
+            constexpr bool kInc = sizeof(R) == 4;
+            for (int k = k0; k < k1; ++k) {
+                CellPsi<R> ps;
+                ps.sz = -1;
+                if (active && interior) load_psi_d(a, i, j, k, sx, sy, ps);
+                const int c = (k * a.ny + j) * a.nxp + i;
+                R ex = R(0), ey = R(0), ez = R(0);
+                if (active && interior && lossy) {
+                    ex = a.f.ex[c];
+                    ey = a.f.ey[c];
+                    ez = a.f.ez[c];
+                }
+                bool ok = true;
+                if (k == k0) ok = mbar_wait(&full[0], 0);
+                ok = ok && mbar_wait(&full[(k - k0 + 1) % G::ES], ((k - k0 + 1) / G::ES) & 1);
+                if (ok && active) {
+                    const unsigned char* bp = stage(k - 1);
+                    const unsigned char* bc = stage(k);
+                    const R* Hxp = reinterpret_cast<const R*>(bp);
+                    const R* Hyp = reinterpret_cast<const R*>(bp + HB);
+                    const R* Hx = reinterpret_cast<const R*>(bc);
+                    const R* Hy = reinterpret_cast<const R*>(bc + HB);
+                    const R* Hz = reinterpret_cast<const R*>(bc + 2 * HB);
+                    const R* Ds = reinterpret_cast<const R*>(bc + 3 * HB);
+                    R dx = Ds[oo], dy = Ds[OB / sizeof(R) + oo], dz = Ds[2 * (OB / sizeof(R)) + oo];
+                    R ix = R(0), iy = R(0), iz = R(0);
+                    R& ux = kInc ? ix : dx;
+                    R& uy = kInc ? iy : dy;
+                    R& uz = kInc ? iz : dz;
+                    if (interior) {
+                        d_update<R, false>(a, i, j, k, sx, sy, Hx[ho], Hy[ho], Hz[ho], Hxp[ho], Hyp[ho], Hz[ho - G::BX],
+                                           Hx[ho - G::BX], Hz[ho - 1], Hy[ho - 1], ps, ux, uy, uz);
+                        if (lossy) { /* fdtd.c:3349-3353 */
+                            const R* q = m.eps_im;
+                            ux -= q[0] * ex + q[1] * ey + q[2] * ez;
+                            uy -= q[3] * ex + q[4] * ey + q[5] * ez;
+                            uz -= q[6] * ex + q[7] * ey + q[8] * ez;
+                        }
+                    }
+                    if constexpr (kInc) {
+                        dx += ix;
+                        dy += iy;
+                        dz += iz;
+                    }
+                    e_update<R, false, NAMAX>(a, m, c, dx, dy, dz, ix, iy, iz, ex, ey, ez);
+                    a.f.dx[c] = dx;
+                    a.f.dy[c] = dy;
+                    a.f.dz[c] = dz;
+                    a.f.ex[c] = ex;
+                    a.f.ey[c] = ey;
+                    a.f.ez[c] = ez;
+                }
+                if (__syncthreads_or(!ok)) {
+                    if (tid == 0) atomicExch(a.err, 1);
+                    break;
+                }
+                if (tid == 0 && k - 1 + G::ES <= k1 - 1) {
+                    fence_proxy_async_smem();
+                    issue(k - 1 + G::ES);
+                }
+            }
+            return;
+        }
+    }
     if (pm == kPlainTensor) {
         /* one lossy or anisotropic material (no ADE, ions or source): the
          * general path's D update with the eps'' term and E = eps^-1 D in
