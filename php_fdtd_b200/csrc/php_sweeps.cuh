@@ -414,12 +414,20 @@ struct IonCoefParam {
     __device__ __forceinline__ R dmm(int q, int p) const { return a.ion_k[kIonKD + q * kIonKQ + p]; }
 };
 
+/* A cell's pool slot, read ahead of the stage wait by a caller that knows
+ * the cell's material. */
+struct IonPre {
+    int64_t slot;
+};
+
 /* D -> E, ADE and ions for one cell (fdtd.c:3404-3528).  ex..ez hold E^n on
  * entry (lab frame) and E^{n+1} on return; dx..dz are D^{n+1}; ix..iz are
- * D^{n+1} - D^n as summed before rounding into D (FP32 only). */
+ * D^{n+1} - D^n as summed before rounding into D (FP32 only).  pre: the
+ * slot already read, or null. */
 template <typename R, bool STRICT, int NAMAX>
 __device__ __forceinline__ void e_update(const StepArgs<R>& a, const MatCoef<R>& m, int c,
-                                         R dx, R dy, R dz, R ix, R iy, R iz, R& ex, R& ey, R& ez)
+                                         R dx, R dy, R dz, R ix, R iy, R iz, R& ex, R& ey, R& ez,
+                                         const IonPre* pre = nullptr)
 {
     const int flags = m.flags;
     if constexpr (!STRICT) {
@@ -432,7 +440,8 @@ __device__ __forceinline__ void e_update(const StepArgs<R>& a, const MatCoef<R>&
         }
     }
     int64_t slot = -1;
-    if (flags & (kAde | kAtoms)) slot = a.slot[c];
+    if (pre) slot = pre->slot;
+    else if (flags & (kAde | kAtoms)) slot = a.slot[c];
     const int64_t ns = a.nslot;
 
     /* P_ion = QeZV . r^n in the crystal frame (fdtd.c:3418-3427).  With

@@ -434,8 +434,12 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
             /* the few-atom material alone (no ADE, no source): the general
              * path's D update and D -> E with the fused ion update, its
              * material record and ion coefficients from the kernel
-             * parameters */
+             * parameters, the cell's slot (and, held in registers, its r
+             * and v) read before the stage wait */
             const MatCoef<R>& m = a.amc;
+            constexpr int QN = 3 * NAMAX;
+            constexpr bool VREG = QN * (int)sizeof(R) <= kIonRegBytes;
+            const int n3 = 3 * m.natom;
             const bool active = (i < a.nx) && (j < a.ny);
             const bool interior = (i >= 1 && i < a.nx - 1 && j >= 1 && j < a.ny - 1);
             const int sx = active ? ldg(a.tx.slot + i) : -1;
@@ -452,6 +456,21 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
                     ex = a.f.ex[c];
                     ey = a.f.ey[c];
                     ez = a.f.ez[c];
+                }
+                IonPre ip;
+                ip.slot = -1;
+                if (active) {
+                    ip.slot = a.slot[c];
+                    /* r and v into L1 ahead of their reads in e_update */
+#pragma unroll
+                    for (int q = 0; q < QN; ++q) {
+                        const int64_t o = VREG ? (int64_t)((uint32_t)q * (uint32_t)a.nslot + (uint32_t)ip.slot)
+                                               : (int64_t)q * a.nslot + ip.slot;
+                        if (q < n3) {
+                            asm volatile("prefetch.global.L1 [%0];" ::"l"(a.r + o));
+                            asm volatile("prefetch.global.L1 [%0];" ::"l"(a.v + o));
+                        }
+                    }
                 }
                 bool ok = true;
                 if (k == k0) ok = mbar_wait(&full[0], 0);
@@ -485,7 +504,7 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
                         dy += iy;
                         dz += iz;
                     }
-                    e_update<R, false, NAMAX>(a, m, c, dx, dy, dz, ix, iy, iz, ex, ey, ez);
+                    e_update<R, false, NAMAX>(a, m, c, dx, dy, dz, ix, iy, iz, ex, ey, ez, &ip);
                     a.f.dx[c] = dx;
                     a.f.dy[c] = dy;
                     a.f.dz[c] = dz;
