@@ -659,7 +659,8 @@ template <typename R, bool STRICT, int NAMAX>
 __device__ __forceinline__ void e_cell_values(const StepArgs<R>& a, int i, int j, int k, int c, bool interior, int sx,
                                               int sy, R hx0, R hy0, R hz0, R hxk, R hyk, R hz_jm, R hx_jm, R hz_im,
                                               R hy_im, R& dx, R& dy, R& dz, int mid, const MatCoef<R>* mcs,
-                                              const CellPsi<R>* pre, R& ex_out, R& ey_out, R& ez_out)
+                                              const CellPsi<R>* pre, R& ex_out, R& ey_out, R& ez_out,
+                                              const IonPre* ipre = nullptr)
 {
     const R* __restrict__ exp_ = a.f.ex;
     const R* __restrict__ eyp = a.f.ey;
@@ -723,7 +724,7 @@ __device__ __forceinline__ void e_cell_values(const StepArgs<R>& a, int i, int j
         ey = iso * dy;
         ez = iso * dz;
     } else {
-        e_update<R, STRICT, NAMAX>(a, *mp, c, dx, dy, dz, ix, iy, iz, ex, ey, ez);
+        e_update<R, STRICT, NAMAX>(a, *mp, c, dx, dy, dz, ix, iy, iz, ex, ey, ez, ipre);
     }
     ex_out = ex;
     ey_out = ey;
@@ -734,11 +735,12 @@ __device__ __forceinline__ void e_cell_values(const StepArgs<R>& a, int i, int j
 template <typename R, bool STRICT, int NAMAX>
 __device__ __forceinline__ void e_cell(const StepArgs<R>& a, int i, int j, int k, int c, bool interior, int sx, int sy,
                                        R hx0, R hy0, R hz0, R hxk, R hyk, R hz_jm, R hx_jm, R hz_im, R hy_im, R dx, R dy,
-                                       R dz, int mid, const MatCoef<R>* mcs, const CellPsi<R>* pre)
+                                       R dz, int mid, const MatCoef<R>* mcs, const CellPsi<R>* pre,
+                                       const IonPre* ipre = nullptr)
 {
     R ex, ey, ez;
     e_cell_values<R, STRICT, NAMAX>(a, i, j, k, c, interior, sx, sy, hx0, hy0, hz0, hxk, hyk, hz_jm, hx_jm, hz_im, hy_im,
-                                    dx, dy, dz, mid, mcs, pre, ex, ey, ez);
+                                    dx, dy, dz, mid, mcs, pre, ex, ey, ez, ipre);
     a.f.dx[c] = dx;
     a.f.dy[c] = dy;
     a.f.dz[c] = dz;

@@ -58,6 +58,11 @@ constexpr uint32_t kWaitLimit = 1u << 24;
 #ifndef PHP_PSI_EARLY_E
 #define PHP_PSI_EARLY_E 1
 #endif
+/* the general path of the FP32 fused sweep reads pool slots one plane ahead
+ * (in FP64 the extra live values spill) */
+#ifndef PHP_SLOT_AHEAD
+#define PHP_SLOT_AHEAD 1
+#endif
 
 /* Tensor maps of the device arrays (3-D: x, y, plane; planes count from the
  * low halo plane of the field arrays). */
@@ -711,12 +716,31 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
     const bool interior = (i >= 1 && i < a.nx - 1 && j >= 1 && j < a.ny - 1);
     const int sx = active ? ldg(a.tx.slot + i) : -1;
     const int sy = active ? ldg(a.ty.slot + j) : -1;
+    /* pool slot of the cell one plane ahead (ADE and atom cells, -1 for the
+     * others): the lines of P, P_old and P_ion of this plane's cell are
+     * requested before the stage wait instead of after the material lookup */
+    const bool slots = PHP_SLOT_AHEAD && sizeof(R) == 4 && a.slot != nullptr && active;
+    int slot_next = slots ? ldg(a.slot + (k0 * a.ny + j) * a.nxp + i) : -1;
 
     for (int k = k0; k < k1; ++k) {
         /* CPML state read before the wait (it does not depend on the stages) */
         CellPsi<R> ps;
         ps.sz = -1;
         if (PHP_PSI_EARLY_E && active && interior) load_psi_d(a, i, j, k, sx, sy, ps);
+        IonPre ip;
+        ip.slot = slot_next;
+        if (slots && k + 1 < k1) slot_next = ldg(a.slot + ((k + 1) * a.ny + j) * a.nxp + i);
+        if (ip.slot >= 0) {
+            const int64_t ns = a.nslot;
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                if (a.P) {
+                    asm volatile("prefetch.global.L1 [%0];" ::"l"(a.P + q * ns + ip.slot));
+                    asm volatile("prefetch.global.L1 [%0];" ::"l"(a.Po + q * ns + ip.slot));
+                }
+                if (!STRICT && NAMAX == 0 && a.pr) asm volatile("prefetch.global.L1 [%0];" ::"l"(a.pr + q * ns + ip.slot));
+            }
+        }
         bool ok = true;
         if (k == k0) ok = mbar_wait(&full[0], 0);
         ok = ok && mbar_wait(&full[(k - k0 + 1) % G::ES], ((k - k0 + 1) / G::ES) & 1);
@@ -736,7 +760,7 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
             const int c = (k * a.ny + j) * a.nxp + i;
             e_cell<R, STRICT, NAMAX>(a, i, j, k, c, interior, sx, sy, Hx[ho], Hy[ho], Hz[ho], Hxp[ho], Hyp[ho],
                                      Hz[ho - G::BX], Hx[ho - G::BX], Hz[ho - 1], Hy[ho - 1], Dx[oo], Dy[oo], Dz[oo], M[oo],
-                                     mcs, &ps);
+                                     mcs, &ps, slots ? &ip : nullptr);
         }
         /* every thread is done with plane k-1: its stage takes plane k-1 + stages */
         if (__syncthreads_or(!ok)) {
