@@ -290,6 +290,29 @@ __device__ __forceinline__ void load_psi_d(const StepArgs<R>& a, int i, int j, i
     }
 }
 
+/* the lines load_psi_d reads at plane k, requested into L1 a plane ahead */
+template <typename R>
+__device__ __forceinline__ void prefetch_psi_d(const StepArgs<R>& a, int i, int j, int k, int sx, int sy)
+{
+    const int L2 = 2 * a.L;
+    if (sx >= 0) {
+        const int q = (k * a.ny + j) * L2 + sx;
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(a.psi.dxy + q));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(a.psi.dxz + q));
+    }
+    if (sy >= 0) {
+        const int q = (k * L2 + sy) * a.nxp + i;
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(a.psi.dyx + q));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(a.psi.dyz + q));
+    }
+    const int sz = ldg_nh(a.tz.slot + k);
+    if (sz >= 0) {
+        const int q = (sz * a.ny + j) * a.nxp + i;
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(a.psi.dzx + q));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(a.psi.dzy + q));
+    }
+}
+
 /* D sweep (fdtd.c:3238-3343) for one interior cell; hx0..hz0 are H at the
  * cell, hxk/hyk at k-1, hz_jm/hx_jm at j-1, hz_im/hy_im at i-1; ps holds the
  * old psi values (load_psi_d). */

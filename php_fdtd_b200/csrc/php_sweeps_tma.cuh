@@ -58,11 +58,22 @@ constexpr uint32_t kWaitLimit = 1u << 24;
 #ifndef PHP_PSI_EARLY_E
 #define PHP_PSI_EARLY_E 1
 #endif
+/* the CPML loops request the psi lines of the next plane into L1: both H
+ * sweeps and the FP64 fused sweep (the FP32 fused sweep measured slower) */
+#ifndef PHP_PSI_AHEAD
+#define PHP_PSI_AHEAD 1
+#endif
+#ifndef PHP_PSI_AHEAD_E32
+#define PHP_PSI_AHEAD_E32 0
+#endif
 /* the general path of the FP32 fused sweep reads pool slots one plane ahead
  * (in FP64 the extra live values spill) */
 #ifndef PHP_SLOT_AHEAD
 #define PHP_SLOT_AHEAD 1
 #endif
+
+template <typename R>
+constexpr bool kPsiAheadE = PHP_PSI_AHEAD && (sizeof(R) == 8 || PHP_PSI_AHEAD_E32);
 
 /* Tensor maps of the device arrays (3-D: x, y, plane; planes count from the
  * low halo plane of the field arrays). */
@@ -276,6 +287,25 @@ __global__ void __launch_bounds__(kBlockX * kBlockY) h_sweep_tma(const __grid_co
             }
         };
         if constexpr (early) load_psi();
+        if (PHP_PSI_AHEAD && !STRICT && active && k + 1 < k1) {
+            /* the lines of plane k + 1 requested into L1 a plane ahead */
+            const int sz1 = ldg_nh(a.tz.slot + k + 1);
+            if (sx >= 0) {
+                const int q = ((k + 1) * ny + j) * L2 + sx;
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(a.psi.hxy + q));
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(a.psi.hxz + q));
+            }
+            if (sy >= 0) {
+                const int q = ((k + 1) * L2 + sy) * nxp + i;
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(a.psi.hyx + q));
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(a.psi.hyz + q));
+            }
+            if (sz1 >= 0) {
+                const int q = (sz1 * ny + j) * nxp + i;
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(a.psi.hzx + q));
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(a.psi.hzy + q));
+            }
+        }
         R khz = R(0);
         if constexpr (!STRICT) khz = ldg_nh(a.tz.kh + k);
 
@@ -455,6 +485,7 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
                 CellPsi<R> ps;
                 ps.sz = -1;
                 if (active && interior) load_psi_d(a, i, j, k, sx, sy, ps);
+                if (kPsiAheadE<R> && active && interior && k + 1 < k1) prefetch_psi_d(a, i, j, k + 1, sx, sy);
                 const int c = (k * a.ny + j) * a.nxp + i;
                 R ex = R(0), ey = R(0), ez = R(0);
                 if (active && interior && lossy) {
@@ -546,6 +577,7 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
             CellPsi<R> ps;
             ps.sz = -1;
             if (active && interior) load_psi_d(a, i, j, k, sx, sy, ps);
+            if (kPsiAheadE<R> && active && interior && k + 1 < k1) prefetch_psi_d(a, i, j, k + 1, sx, sy);
             const int c = (k * a.ny + j) * a.nxp + i;
             R ex = R(0), ey = R(0), ez = R(0);
             if (active && interior && lossy) {
@@ -625,6 +657,7 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
             CellPsi<R> ps;
             ps.sz = -1;
             if (active && interior) load_psi_d(a, i, j, k, sx, sy, ps);
+            if (kPsiAheadE<R> && active && interior && k + 1 < k1) prefetch_psi_d(a, i, j, k + 1, sx, sy);
             bool ok = true;
             if (k == k0) ok = mbar_wait(&full[0], 0);
             ok = ok && mbar_wait(&full[(k - k0 + 1) % G::ES], ((k - k0 + 1) / G::ES) & 1);
@@ -727,6 +760,7 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
         CellPsi<R> ps;
         ps.sz = -1;
         if (PHP_PSI_EARLY_E && active && interior) load_psi_d(a, i, j, k, sx, sy, ps);
+        if (kPsiAheadE<R> && !STRICT && active && interior && k + 1 < k1) prefetch_psi_d(a, i, j, k + 1, sx, sy);
         IonPre ip;
         ip.slot = slot_next;
         if (slots && k + 1 < k1) slot_next = ldg(a.slot + ((k + 1) * a.ny + j) * a.nxp + i);
