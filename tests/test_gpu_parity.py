@@ -71,7 +71,7 @@ def test_fp32_close_to_reference(name, golden_case):
         if np.abs(ref).max() > 0:
             errs.append(H.rel_l2(res["slices"][s], ref))
     # the first samples of a pulse are a few cells wide and dominated by
-    # round-off; judge the slices of the last half of the run
+    # round-off; the check takes the slices of the last half of the run
     tail = errs[len(errs) // 2:]
     assert tail and max(tail) <= FP32_TOL, (name, errs)
 
