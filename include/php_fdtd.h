@@ -314,7 +314,7 @@ int php_profile_read(php_ctx* ctx, double* ms, int64_t* launches);
 
 /* No counterpart in the reference.  For callers that cannot allocate device
  * memory at the moment they need the field maxima: a divergence check on a
- * device whose memory is full (a large domain takes most of the HBM, and a
+ * device whose memory is full (resident domains take most of the HBM, and a
  * failing cudaMalloc would hide the real state), a host whose own allocator
  * owns all device memory, or a latency-critical loop where cudaMalloc /
  * cudaFree would synchronise the device.
@@ -326,9 +326,12 @@ int php_profile_read(php_ctx* ctx, double* ms, int64_t* launches);
  * default stream).  It allocates nothing: its scratch is a fixed 256 KB
  * array inside the library, which every GPU that loads the library holds
  * until the process exits.  n above PHP_NOALLOC_MAX_CELLS is rejected with
- * PHP_ERR_INPUT.  The first call on each device looks up the scratch
- * address on that device (make it before any stream capture); calls that
- * overlap on the GPU share the scratch and race, so serialise them. */
+ * PHP_ERR_INPUT; a larger domain is reduced in pieces of at most that many
+ * cells, one call per piece.  The first call on each device looks up the
+ * scratch address on that device, and so does the first call after the
+ * device's context was destroyed and made anew (cudaDeviceReset); make
+ * those calls before any stream capture.  Calls that overlap on the GPU
+ * share the scratch and race, so serialise them. */
 #define PHP_NOALLOC_MAX_CELLS 67108864 /* 2^26 cells, e.g. 512 x 512 x 256 */
 int php_field_maxima_noalloc(const double* ex, const double* ey, const double* ez, int64_t n,
                              double* out2, void* stream);

@@ -18,7 +18,8 @@
  *     messages of each pair in the order they are received.
  * A rank that calls MPI_Abort marks the region; spinning ranks then exit.
  * Children die with rank 0 (PR_SET_PDEATHSIG); MPI_Finalize on rank 0
- * waits for them.
+ * waits for them.  PHP_WIDE_OUTPUT widens the outputs as in the one-rank
+ * stub (wide_output.h).
  */
 #ifndef PHP_ORACLE_MPI_SHM_H
 #define PHP_ORACLE_MPI_SHM_H
@@ -47,7 +48,11 @@ typedef struct { int MPI_SOURCE, MPI_TAG, MPI_ERROR; } MPI_Status;
 #define MPI_CHAR 1
 #define MPI_BYTE 1001
 #define MPI_INT 4
+#ifdef PHP_WIDE_OUTPUT
+#define MPI_FLOAT 2008 /* the slice buffers are double under PHP_WIDE_OUTPUT */
+#else
 #define MPI_FLOAT 1004
+#endif
 #define MPI_DOUBLE 8
 #define MPI_UNSIGNED_LONG_LONG 1008
 #define MPI_MAX 1
@@ -203,6 +208,10 @@ static inline void php_shm_reduce_into(void* r, int n, MPI_Datatype t, MPI_Op op
             } else if (t == MPI_UNSIGNED_LONG_LONG) {
                 unsigned long long* d = (unsigned long long*)r + i;
                 const unsigned long long v = ((const unsigned long long*)x)[i];
+                *d = op == MPI_MAX ? (v > *d ? v : *d) : *d + v;
+            } else if (t == MPI_FLOAT && sz == sizeof(double)) {
+                double* d = (double*)r + i;
+                const double v = ((const double*)x)[i];
                 *d = op == MPI_MAX ? (v > *d ? v : *d) : *d + v;
             } else if (t == MPI_FLOAT) {
                 float* d = (float*)r + i;
@@ -361,5 +370,9 @@ static inline double MPI_Wtime(void)
     clock_gettime(CLOCK_MONOTONIC, &ts);
     return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
 }
+
+#ifdef PHP_WIDE_OUTPUT
+#include "../wide_output.h"
+#endif
 
 #endif

@@ -14,13 +14,7 @@
  * they abort loudly.
  *
  * PHP_WIDE_OUTPUT (compile-time) widens the reference's OUTPUTS without
- * touching its arithmetic, so results can be compared at 1e-10 and below:
- *   - `float` becomes `double` for the code after this header, which only
- *     affects the field-slice buffers (fdtd.c:1050-1092, 1115-1261,
- *     1308-1383): slices are written as float64 instead of float32;
- *   - every `%e`/`%.Ne` conversion of fprintf becomes `%.17e`, which widens
- *     monitor_point.dat, full_monitor.dat (fdtd.c:3754, 3839, 3865) and
- *     source.txt (fdtd.c:3360, 3367) to round-trip precision.
+ * touching its arithmetic (float64 slices, %.17e monitors): wide_output.h.
  */
 #ifndef PHP_ORACLE_MPI_STUB_H
 #define PHP_ORACLE_MPI_STUB_H
@@ -43,7 +37,11 @@ typedef struct { int MPI_SOURCE, MPI_TAG, MPI_ERROR; } MPI_Status;
 #define MPI_CHAR 1
 #define MPI_BYTE 1001
 #define MPI_INT 4
+#ifdef PHP_WIDE_OUTPUT
+#define MPI_FLOAT 2008 /* the slice buffers are double under PHP_WIDE_OUTPUT */
+#else
 #define MPI_FLOAT 1004
+#endif
 #define MPI_DOUBLE 8
 #define MPI_UNSIGNED_LONG_LONG 1008
 
@@ -96,31 +94,7 @@ static inline double MPI_Wtime(void)
 }
 
 #ifdef PHP_WIDE_OUTPUT
-/* Rewrites every %e conversion (any flags/width/precision) to %.17e. */
-static inline int php_wide_fprintf(FILE* f, const char* fmt, ...)
-{
-    char wide[1024];
-    size_t o = 0;
-    for (const char* p = fmt; *p && o + 8 < sizeof(wide); ) {
-        if (*p != '%') { wide[o++] = *p++; continue; }
-        const char* q = p + 1;
-        if (*q == '%') { wide[o++] = '%'; wide[o++] = '%'; p = q + 1; continue; }
-        while (*q && strchr("-+ #0123456789.", *q)) q++;
-        if (*q == 'e') {
-            memcpy(wide + o, "%.17e", 5); o += 5; p = q + 1;
-        } else {
-            while (p <= q && *p && o + 1 < sizeof(wide)) wide[o++] = *p++;
-        }
-    }
-    wide[o] = '\0';
-    va_list ap;
-    va_start(ap, fmt);
-    int n = vfprintf(f, wide, ap);
-    va_end(ap);
-    return n;
-}
-#define fprintf php_wide_fprintf
-#define float double
+#include "../wide_output.h"
 #endif
 
 #endif

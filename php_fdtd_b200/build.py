@@ -4,7 +4,8 @@
   php_fdtd_b200/libphphost.so   C host layer (include/php_host.h), no CUDA
   php_fdtd_b200/fdtd_b200       drop-in solver executable
   oracle/liboracle.so           CPU restatement (test infrastructure)
-  oracle/_ref/*                 the reference solver, when its sources exist
+  oracle/_ref/*                 the reference solver and post-processor, when
+                                PHP_REFERENCE_DIR names the reference checkout
 
 Run ``python -m php_fdtd_b200.build`` or call ``build()``.  Each target is
 rebuilt only when one of its inputs is newer.
@@ -23,7 +24,6 @@ INC = ROOT / "include"
 CSRC = PKG / "csrc"
 HOST = PKG / "host"
 ORACLE = ROOT / "oracle"
-REFERENCE_SRC = Path(os.environ.get("PHP_REFERENCE_DIR", "/root/reference"))
 
 NVCC_ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -82,11 +82,18 @@ def build_cli(verbose: bool = False) -> Path:
     return out
 
 
+def reference_dir() -> Path | None:
+    """The reference checkout named by PHP_REFERENCE_DIR, if it holds fdtd.c."""
+    v = os.environ.get("PHP_REFERENCE_DIR", "")
+    return Path(v) if v and (Path(v) / "fdtd.c").exists() else None
+
+
 def build_oracle(verbose: bool = False) -> None:
     targets = ["restatement"]
-    if (REFERENCE_SRC / "fdtd.c").exists():
+    ref = reference_dir()
+    if ref is not None:
         targets.append("ref")
-    cmd = ["make", "-s", "-C", ORACLE, f"REF={REFERENCE_SRC}", *targets]
+    cmd = ["make", "-s", "-C", ORACLE, *([f"REF={ref}"] if ref is not None else []), *targets]
     _run(cmd, verbose)
 
 

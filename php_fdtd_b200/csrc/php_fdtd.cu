@@ -138,8 +138,7 @@ struct php_ctx {
 
     std::vector<DftPlane> dft;
 
-    /* sweep kernels: TMA plane pipeline (default) or register prefetch */
-    bool use_tma = true;
+    /* TMA maps of the sweep kernels */
     TmaMaps maps;
     int32_t* err_flag = nullptr;
 
@@ -667,16 +666,13 @@ static void launch_step_t(php_ctx* ctx, int s_local, int& launches)
     const bool do_h = ctx->step_part & 1, do_e = ctx->step_part & 2;
     if (do_h) {
         prof_mark(ctx, s_local, 0, 0);
-        if (ctx->use_tma) h_sweep_tma<R, STRICT><<<grid, block, TmaGeom<R>::H_SMEM, ctx->stream>>>(a, ctx->maps);
-        else h_sweep<R, STRICT><<<grid, block, 0, ctx->stream>>>(a);
+        h_sweep_tma<R, STRICT><<<grid, block, TmaGeom<R>::H_SMEM, ctx->stream>>>(a, ctx->maps);
         prof_mark(ctx, s_local, 0, 1);
         launches++;
     }
     if (!do_e) return;
     prof_mark(ctx, s_local, 1, 0);
-    if (ctx->use_tma)
-        e_sweep_tma<R, STRICT, NA><<<grid, block, TmaGeom<R>::E_SMEM + a.nmat * sizeof(MatCoef<R>), ctx->stream>>>(a, ctx->maps);
-    else e_sweep<R, STRICT, NA><<<grid, block, 0, ctx->stream>>>(a);
+    e_sweep_tma<R, STRICT, NA><<<grid, block, TmaGeom<R>::E_SMEM + a.nmat * sizeof(MatCoef<R>), ctx->stream>>>(a, ctx->maps);
     prof_mark(ctx, s_local, 1, 1);
     launches++;
     if constexpr (!STRICT && NA == 0) {
@@ -1406,16 +1402,11 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
         ctx->kdp[2] = d.dt / (d.dz * 1.0);
     }
 
-    /* sweep kernels: the TMA plane pipeline unless PHP_SWEEP=prefetch asks
-     * for the register-prefetch kernels (kept for A/B timing) */
-    const char* sw = getenv("PHP_SWEEP");
-    ctx->use_tma = !(sw && !strcmp(sw, "prefetch"));
+    /* sweep kernels: the TMA plane pipeline */
     if ((rc = dalloc(ctx, (void**)&ctx->err_flag, sizeof(int32_t)))) return rc;
-    if (ctx->use_tma) {
-        rc = ctx->prec == PHP_PREC_FP32 ? make_maps<float>(ctx) : make_maps<double>(ctx);
-        if (!rc) rc = pick_step(ctx).prepare(ctx);
-        if (rc) return rc;
-    }
+    rc = ctx->prec == PHP_PREC_FP32 ? make_maps<float>(ctx) : make_maps<double>(ctx);
+    if (!rc) rc = pick_step(ctx).prepare(ctx);
+    if (rc) return rc;
 
     /* per-step inputs, scratch, staging */
     if ((rc = alloc_step_inputs(ctx, std::max(1, ctx->nsrc_active)))) return rc;

@@ -4,9 +4,12 @@
  * php_diagnostics reduces |E| and |Ex| in two passes through a scratch
  * buffer that php_create allocates.  Some callers cannot allocate device
  * memory when they need these maxima:
- *   - a divergence or health check that runs when HBM is exhausted (a
- *     1024 x 1024 x 512 domain fills most of the 180 GB), where one more
- *     cudaMalloc is exactly what fails;
+ *   - a divergence or health check that runs when HBM is exhausted (many
+ *     resident domains, or one large domain with its lattice state, fill
+ *     most of the 180 GB), where one more cudaMalloc is exactly what fails;
+ *     a domain above PHP_NOALLOC_MAX_CELLS (2^26 cells) is reduced in
+ *     pieces of at most that many cells, one call per piece, the caller
+ *     keeping the larger results;
  *   - hosts whose allocator owns all device memory (a framework caching
  *     allocator, a fixed memory pool) and forbid allocations behind its back;
  *   - latency-critical loops, where cudaMalloc/cudaFree would synchronise the
@@ -17,6 +20,7 @@
  */
 #include "php_fdtd.h"
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -30,14 +34,49 @@ constexpr int kCellsPerThread = 16;
 constexpr int64_t kCellsPerBlock = (int64_t)kThreads * kCellsPerThread;
 constexpr int kMaxBlocks = PHP_NOALLOC_MAX_CELLS / (int)(kThreads * kCellsPerThread);
 constexpr int kMaxDevices = 64;
+/* pass 1 writes one partial per kCellsPerBlock cells: the cap must be a
+ * whole number of blocks, or its last block would write past the array */
+static_assert(PHP_NOALLOC_MAX_CELLS % kCellsPerBlock == 0, "PHP_NOALLOC_MAX_CELLS must be a multiple of 4096");
 
 /* One partial (max |E|, max |Ex|) per block of the first pass.  Pass 1
  * writes every entry that pass 2 reads, so nothing needs clearing between
  * calls; calls that overlap on the GPU (two streams at once) race on it. */
 static __device__ __align__(256) double g_partials[kMaxBlocks][2];
 
+/* The device address of g_partials, per device, with the id of the CUDA
+ * context it was resolved in: a context destroyed and made anew (a
+ * cudaDeviceReset by the caller) gets a new id, and the address is looked up
+ * again in it. */
+struct Resolved {
+    unsigned long long ctx_id = 0;
+    double (*ptr)[2] = nullptr;
+};
 std::mutex g_mu;
-double (*g_partials_dev[kMaxDevices])[2] = {};
+Resolved g_resolved[kMaxDevices];
+
+typedef CUresult (*ctx_current_fn)(CUcontext*);
+typedef CUresult (*ctx_id_fn)(CUcontext, unsigned long long*);
+
+/* id of the context current on this thread; false if there is none yet */
+static bool current_ctx_id(unsigned long long* id)
+{
+    static ctx_current_fn get_current = nullptr;
+    static ctx_id_fn get_id = nullptr;
+    if (!get_current || !get_id) {
+        void *a = nullptr, *b = nullptr;
+        cudaDriverEntryPointQueryResult qa, qb;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) != cudaSuccess ||
+            qa != cudaDriverEntryPointSuccess || !a ||
+            cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) != cudaSuccess ||
+            qb != cudaDriverEntryPointSuccess || !b)
+            return false;
+        get_current = reinterpret_cast<ctx_current_fn>(a);
+        get_id = reinterpret_cast<ctx_id_fn>(b);
+    }
+    CUcontext c = nullptr;
+    if (get_current(&c) != CUDA_SUCCESS || !c) return false;
+    return get_id(c, id) == CUDA_SUCCESS;
+}
 
 /* sqrt(Ex^2 + Ey^2 + Ez^2) in the order of fdtd.c:3542-3544 and |Ex|; the
  * comparisons skip NaN as the reference's `>` tests do. */
@@ -110,15 +149,21 @@ extern "C" int php_field_maxima_noalloc(const double* ex, const double* ey, cons
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return PHP_ERR_CUDA;
     double(*partials)[2] = nullptr;
     {
-        /* first call on this device: resolve the device address of the
-         * file-scope array (its host-side name is only a stand-in) */
+        /* first call on this device, or in a new context of it: resolve the
+         * device address of the file-scope array (its host-side name is only
+         * a stand-in), with the device current */
         std::lock_guard<std::mutex> lock(g_mu);
-        if (!g_partials_dev[dev]) {
+        unsigned long long id = 0;
+        const bool known = current_ctx_id(&id);
+        Resolved& r = g_resolved[dev];
+        if (!known || !r.ptr || r.ctx_id != id) {
             void* p = nullptr;
             if (cudaGetSymbolAddress(&p, g_partials) != cudaSuccess || !p) return PHP_ERR_CUDA;
-            g_partials_dev[dev] = reinterpret_cast<double(*)[2]>(p);
+            if (!current_ctx_id(&id)) return PHP_ERR_CUDA;
+            r.ptr = reinterpret_cast<double(*)[2]>(p);
+            r.ctx_id = id;
         }
-        partials = g_partials_dev[dev];
+        partials = r.ptr;
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int nblocks = (int)((n + kCellsPerBlock - 1) / kCellsPerBlock);

@@ -1,199 +1,17 @@
 /*
- * php_sweeps.cuh -- the two sweeps of one PhP_FDTD time step on sm_100a.
+ * php_sweeps.cuh -- the per-cell physics of one PhP_FDTD time step, shared by
+ * the TMA plane-ring sweeps of php_sweeps_tma.cuh:
  *
- *   h_sweep   H += dt (curl E / kappa + psi_H)          fdtd.c:3123-3231
- *   e_sweep   D += dt (curl H / kappa + psi_D) - eps''  fdtd.c:3238-3356
- *             + sources                                 fdtd.c:3363-3400
- *             D -> E (rotation, eps^-1 or ADE, loss)    fdtd.c:3404-3503
- *             ion equations of motion                   fdtd.c:3505-3528
+ *   d_update        D += dt (curl H / kappa + psi_D) - eps''  fdtd.c:3238-3356
+ *   e_cell_values   D -> E (rotation, eps^-1 or ADE, loss)    fdtd.c:3404-3503
+ *   e_update        tensor ADE and the ion equations of motion fdtd.c:3463-3528
  *
- * Both are streaming kernels bound by HBM bandwidth.  A thread owns one
- * (i, j) column of a z chunk and marches up in k.  Three things keep enough
- * bytes in flight to run at the copy bandwidth:
- *   - the values of plane k+1 are loaded into registers while plane k is
- *     computed (the loads of one iteration overlap the math of the previous);
- *   - the z neighbour is carried in registers (k+1 for H, k-1 for E), the
- *     in-plane neighbours come from L1 (the neighbouring lanes / rows of the
- *     same block loaded them);
- *   - CPML and material coefficients are loaded only inside the branches
- *     that need them, so they never occupy registers across the loop.
+ * CPML and material coefficients are loaded only inside the branches that
+ * need them, so they never occupy registers across the sweeps' loops.
  */
 #pragma once
 
 namespace phpdev {
-
-/* ================================================================ H sweep */
-
-#ifndef PHP_E_MINBLOCKS
-#define PHP_E_MINBLOCKS 4
-#endif
-#ifndef PHP_PREFETCH
-#define PHP_PREFETCH 1
-#endif
-
-/* Values of one plane that stream from HBM: the k+1 E values carried up the
- * column, the own Ez and the H being updated.  In-plane neighbours are
- * loaded inside the iteration (L1 hits). */
-template <typename R>
-struct HIn {
-    R ex1, ey1, ez0, hx, hy, hz;
-};
-
-template <typename R>
-__device__ __forceinline__ void h_fetch(HIn<R>& q, const R* __restrict__ ex, const R* __restrict__ ey,
-                                        const R* __restrict__ ez, const R* __restrict__ hx, const R* __restrict__ hy,
-                                        const R* __restrict__ hz, int c, int P)
-{
-    q.ex1 = ldg(ex + c + P);
-    q.ey1 = ldg(ey + c + P);
-    q.ez0 = ldg(ez + c);
-    q.hx = hx[c];
-    q.hy = hy[c];
-    q.hz = hz[c];
-}
-
-/* fdtd.c:3123-3231.  Cells i < nx-1, j < ny-1, all k.  Cell offsets fit in
- * 32 bits for every grid up to 2^31 cells (1024 x 1024 x 2046). */
-template <typename R, bool STRICT>
-__global__ void __launch_bounds__(kBlockX * kBlockY, 3) h_sweep(const StepArgs<R> a)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= a.nx - 1 || j >= a.ny - 1) return;
-    const int k0 = blockIdx.z * a.zchunk;
-    const int k1 = min(k0 + a.zchunk, a.nz);
-    if (k0 >= k1) return;
-
-    const int L2 = 2 * a.L;
-    const int sx = ldg(a.tx.slot + i);
-    const int sy = ldg(a.ty.slot + j);
-    const int P = (int)a.plane;
-    const int nxp = a.nxp, ny = a.ny;
-    int c = (k0 * ny + j) * nxp + i;
-
-    const R* __restrict__ ex = a.f.ex;
-    const R* __restrict__ ey = a.f.ey;
-    const R* __restrict__ ez = a.f.ez;
-    R* __restrict__ hx = a.f.hx;
-    R* __restrict__ hy = a.f.hy;
-    R* __restrict__ hz = a.f.hz;
-
-    R ex0 = ldg(ex + c), ey0 = ldg(ey + c);
-    HIn<R> cur;
-    h_fetch(cur, ex, ey, ez, hx, hy, hz, c, P);
-    R khx = R(0), khy = R(0);
-    if constexpr (!STRICT) {
-        khx = ldg(a.tx.kh + i);
-        khy = ldg(a.ty.kh + j);
-    }
-
-    for (int k = k0; k < k1; ++k, c += P) {
-#if PHP_PREFETCH
-        HIn<R> nxt = cur;
-        if (k + 1 < k1) h_fetch(nxt, ex, ey, ez, hx, hy, hz, c + P, P);
-#else
-        if (k > k0) h_fetch(cur, ex, ey, ez, hx, hy, hz, c, P);
-#endif
-        const R ezi = ldg(ez + c + 1), eyi = ldg(ey + c + 1);
-        const R ezj = ldg(ez + c + nxp), exj = ldg(ex + c + nxp);
-        const int sz = ldg_nh(a.tz.slot + k);
-
-        if constexpr (STRICT) {
-            const double mu0 = a.mu0;
-            /* fdtd.c:3132-3137 */
-            const double dEy_dz = SOp::div(SOp::sub(cur.ey1, ey0), a.dzs);
-            const double dEz_dy = SOp::div(SOp::sub(ezj, cur.ez0), a.dys);
-            const double dEz_dx = SOp::div(SOp::sub(ezi, cur.ez0), a.dxs);
-            const double dEx_dz = SOp::div(SOp::sub(cur.ex1, ex0), a.dzs);
-            const double dEx_dy = SOp::div(SOp::sub(exj, ex0), a.dys);
-            const double dEy_dx = SOp::div(SOp::sub(eyi, ey0), a.dxs);
-            double pxy = 0.0, pxz = 0.0, pyx = 0.0, pyz = 0.0, pzx = 0.0, pzy = 0.0;
-            double kappa_x = 1.0, kappa_y = 1.0, kappa_z = 1.0;
-            if (sx >= 0) { /* fdtd.c:3143-3170 */
-                kappa_x = ldg_nh(a.tx.kappa + i);
-                const double b = ldg_nh(a.tx.b + i), cc = ldg_nh(a.tx.c + i);
-                const int q = (k * ny + j) * L2 + sx;
-                pxy = a.psi.hxy[q];
-                pxz = a.psi.hxz[q];
-                a.psi.hxy[q] = SOp::add(SOp::mul(b, pxy), SOp::mul(cc, SOp::div(dEz_dx, mu0)));
-                a.psi.hxz[q] = SOp::add(SOp::mul(b, pxz), SOp::mul(cc, SOp::div(-dEy_dx, mu0)));
-            }
-            if (sy >= 0) { /* fdtd.c:3173-3200 */
-                kappa_y = ldg_nh(a.ty.kappa + j);
-                const double b = ldg_nh(a.ty.b + j), cc = ldg_nh(a.ty.c + j);
-                const int q = (k * L2 + sy) * nxp + i;
-                pyx = a.psi.hyx[q];
-                pyz = a.psi.hyz[q];
-                a.psi.hyx[q] = SOp::add(SOp::mul(b, pyx), SOp::mul(cc, SOp::div(-dEz_dy, mu0)));
-                a.psi.hyz[q] = SOp::add(SOp::mul(b, pyz), SOp::mul(cc, SOp::div(dEx_dy, mu0)));
-            }
-            int qz = 0;
-            if (sz >= 0) { /* fdtd.c:3203-3219 */
-                kappa_z = ldg_nh(a.tz.kappa + k);
-                qz = (sz * ny + j) * nxp + i;
-                pzx = a.psi.hzx[qz];
-                pzy = a.psi.hzy[qz];
-            }
-            /* fdtd.c:3222-3224 */
-            const double ux = SOp::add(SOp::add(SOp::add(SOp::div(SOp::div(-dEz_dy, mu0), kappa_y), pyx),
-                                                SOp::div(SOp::div(dEy_dz, mu0), kappa_z)), pzx);
-            const double uy = SOp::add(SOp::add(SOp::add(SOp::div(SOp::div(dEz_dx, mu0), kappa_x), pxy),
-                                                SOp::div(SOp::div(-dEx_dz, mu0), kappa_z)), pzy);
-            const double uz = SOp::add(SOp::add(SOp::add(SOp::div(SOp::div(-dEy_dx, mu0), kappa_x), pxz),
-                                                SOp::div(SOp::div(dEx_dy, mu0), kappa_y)), pyz);
-            hx[c] = SOp::add(cur.hx, SOp::mul(a.dt, ux));
-            hy[c] = SOp::add(cur.hy, SOp::mul(a.dt, uy));
-            hz[c] = SOp::add(cur.hz, SOp::mul(a.dt, uz));
-            if (sz >= 0) { /* fdtd.c:3225-3228 */
-                const double b = ldg_nh(a.tz.b + k), cc = ldg_nh(a.tz.c + k);
-                a.psi.hzx[qz] = SOp::add(SOp::mul(b, pzx), SOp::mul(cc, SOp::div(dEy_dz, mu0)));
-                a.psi.hzy[qz] = SOp::add(SOp::mul(b, pzy), SOp::mul(cc, SOp::div(-dEx_dz, mu0)));
-            }
-        } else {
-            const R dEyz = cur.ey1 - ey0, dEzy = ezj - cur.ez0, dEzx = ezi - cur.ez0;
-            const R dExz = cur.ex1 - ex0, dExy = exj - ex0, dEyx = eyi - ey0;
-            const R khz = ldg_nh(a.tz.kh + k);
-            R ux = -khy * dEzy + khz * dEyz;
-            R uy = khx * dEzx - khz * dExz;
-            R uz = -khx * dEyx + khy * dExy;
-            if (sx >= 0) {
-                const R b = ldg_nh(a.tx.b + i), ch = ldg_nh(a.tx.ch + i);
-                const int q = (k * ny + j) * L2 + sx;
-                const R pxy = a.psi.hxy[q], pxz = a.psi.hxz[q];
-                uy += pxy;
-                uz += pxz;
-                a.psi.hxy[q] = b * pxy + ch * dEzx;
-                a.psi.hxz[q] = b * pxz - ch * dEyx;
-            }
-            if (sy >= 0) {
-                const R b = ldg_nh(a.ty.b + j), ch = ldg_nh(a.ty.ch + j);
-                const int q = (k * L2 + sy) * nxp + i;
-                const R pyx = a.psi.hyx[q], pyz = a.psi.hyz[q];
-                ux += pyx;
-                uz += pyz;
-                a.psi.hyx[q] = b * pyx - ch * dEzy;
-                a.psi.hyz[q] = b * pyz + ch * dExy;
-            }
-            if (sz >= 0) {
-                const R b = ldg_nh(a.tz.b + k), ch = ldg_nh(a.tz.ch + k);
-                const int q = (sz * ny + j) * nxp + i;
-                const R pzx = a.psi.hzx[q], pzy = a.psi.hzy[q];
-                ux += pzx;
-                uy += pzy;
-                a.psi.hzx[q] = b * pzx + ch * dEyz;
-                a.psi.hzy[q] = b * pzy - ch * dExz;
-            }
-            hx[c] = cur.hx + ux;
-            hy[c] = cur.hy + uy;
-            hz[c] = cur.hz + uz;
-        }
-        ex0 = cur.ex1;
-        ey0 = cur.ey1;
-#if PHP_PREFETCH
-        cur = nxt;
-#endif
-    }
-}
 
 /* ================================================================ E sweep */
 
@@ -770,79 +588,6 @@ __device__ __forceinline__ void e_cell(const StepArgs<R>& a, int i, int j, int k
     a.f.ex[c] = ex;
     a.f.ey[c] = ey;
     a.f.ez[c] = ez;
-}
-
-template <typename R>
-struct EIn {
-    R hx, hy, hz, dx, dy, dz;
-    int mid;
-};
-
-template <typename R>
-__device__ __forceinline__ void e_fetch(EIn<R>& q, const R* __restrict__ hx, const R* __restrict__ hy,
-                                        const R* __restrict__ hz, const R* __restrict__ dx, const R* __restrict__ dy,
-                                        const R* __restrict__ dz, const uint8_t* __restrict__ mat, int c)
-{
-    q.hx = ldg(hx + c);
-    q.hy = ldg(hy + c);
-    q.hz = ldg(hz + c);
-    q.dx = dx[c];
-    q.dy = dy[c];
-    q.dz = dz[c];
-    q.mid = ldg(mat + c);
-}
-
-/* fdtd.c:3238-3528 fused: D sweep on the interior (i in [1,nx-1), j in
- * [1,ny-1)), sources, then D -> E / ADE / ions on every cell. */
-template <typename R, bool STRICT, int NAMAX>
-__global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : PHP_E_MINBLOCKS)) e_sweep(const StepArgs<R> a)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= a.nx || j >= a.ny) return;
-    const int k0 = blockIdx.z * a.zchunk;
-    const int k1 = min(k0 + a.zchunk, a.nz);
-    if (k0 >= k1) return;
-    const bool interior = (i >= 1 && i < a.nx - 1 && j >= 1 && j < a.ny - 1);
-    const int sx = ldg(a.tx.slot + i);
-    const int sy = ldg(a.ty.slot + j);
-    const int P = (int)a.plane;
-    int c = (k0 * a.ny + j) * a.nxp + i;
-
-    const R* __restrict__ hx = a.f.hx;
-    const R* __restrict__ hy = a.f.hy;
-    const R* __restrict__ hz = a.f.hz;
-    R* __restrict__ dxp = a.f.dx;
-    R* __restrict__ dyp = a.f.dy;
-    R* __restrict__ dzp = a.f.dz;
-    const uint8_t* __restrict__ mat = a.mat;
-
-    R hxk = ldg(hx + c - P), hyk = ldg(hy + c - P); /* plane k-1 */
-    EIn<R> cur;
-    e_fetch(cur, hx, hy, hz, dxp, dyp, dzp, mat, c);
-
-    for (int k = k0; k < k1; ++k, c += P) {
-#if PHP_PREFETCH
-        EIn<R> nxt = cur;
-        if (k + 1 < k1) e_fetch(nxt, hx, hy, hz, dxp, dyp, dzp, mat, c + P);
-#else
-        if (k > k0) e_fetch(cur, hx, hy, hz, dxp, dyp, dzp, mat, c);
-#endif
-        R hz_jm = R(0), hx_jm = R(0), hz_im = R(0), hy_im = R(0);
-        if (interior) {
-            hz_jm = ldg(hz + c - a.nxp);
-            hx_jm = ldg(hx + c - a.nxp);
-            hz_im = ldg(hz + c - 1);
-            hy_im = ldg(hy + c - 1);
-        }
-        e_cell<R, STRICT, NAMAX>(a, i, j, k, c, interior, sx, sy, cur.hx, cur.hy, cur.hz, hxk, hyk, hz_jm, hx_jm, hz_im,
-                                 hy_im, cur.dx, cur.dy, cur.dz, cur.mid, nullptr, nullptr);
-        hxk = cur.hx;
-        hyk = cur.hy;
-#if PHP_PREFETCH
-        cur = nxt;
-#endif
-    }
 }
 
 } // namespace phpdev

@@ -51,7 +51,11 @@ constexpr uint32_t kWaitLimit = 1u << 24;
 #ifndef PHP_PSI_EARLY_H32
 #define PHP_PSI_EARLY_H32 0
 #endif
-/* resident blocks the fused sweep is compiled for (register budget) */
+/* resident blocks the fused sweep is compiled for (register budget), FP64
+ * and FP32 */
+#ifndef PHP_E_MINBLOCKS
+#define PHP_E_MINBLOCKS 4
+#endif
 #ifndef PHP_E_MINBLOCKS32
 #define PHP_E_MINBLOCKS32 4
 #endif

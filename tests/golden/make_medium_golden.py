@@ -48,4 +48,8 @@ def main(ref: Path):
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    import os
+    arg = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PHP_REFERENCE_DIR", "")
+    if not arg:
+        sys.exit("usage: make_medium_golden.py <reference checkout>  (or set PHP_REFERENCE_DIR)")
+    main(Path(arg))

@@ -144,8 +144,13 @@ def run_inprocess(case_dir: Path, runner: str = "oracle", precision: str = "fp64
 
 
 def rel_l2(a, b) -> float:
-    a = np.asarray(a, dtype=np.float64)
-    b = np.asarray(b, dtype=np.float64)
+    """||a - b|| / ||b||; complex inputs keep their imaginary parts (a
+    running-DFT accumulator is checked in amplitude and phase)."""
+    a = np.asarray(a)
+    b = np.asarray(b)
+    if not (np.iscomplexobj(a) or np.iscomplexobj(b)):
+        a = a.astype(np.float64)
+        b = b.astype(np.float64)
     den = np.linalg.norm(b)
     num = np.linalg.norm(a - b)
     if den == 0.0:

@@ -132,9 +132,13 @@ def test_running_dft_matches_direct_sum(golden_case):
     sim.step(23)
     got, ns = sim.dft_read(pid)
     assert ns == n
+    assert np.iscomplexobj(got) and np.abs(acc.imag).max() > 0
     assert H.rel_l2(got, acc) < 1e-12
+    # the sine part on its own: its sign is the transform's direction
+    assert H.rel_l2(got.imag, acc.imag) < 1e-12
     got32, _ = sim.dft_read(pid32)
     assert H.rel_l2(got32, acc32) < 1e-12
+    assert H.rel_l2(got32.imag, acc32.imag) < 1e-12
 
 
 def test_device_rejects_bad_descriptions(golden_case):
