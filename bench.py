@@ -52,6 +52,10 @@ def parse():
     p.add_argument("--acc-steps", type=int, default=None,
                    help="steps of the FP32-vs-FP64 error run (default: the configuration's tsteps; 0 = skip)")
     p.add_argument("--case-dir", default=None)
+    p.add_argument("--no-largest", action="store_true", help="skip the 1024 x 1024 x 512 (cfg4) sub-object")
+    p.add_argument("--z-chunk", type=int, default=0, help="planes per sweep block (0 = the library's choice)")
+    p.add_argument("--largest-steps", type=int, default=2000,
+                   help="steps of the cfg4 runs whose FP32-vs-FP64 error is reported")
     p.add_argument("--requests", type=int, default=256, help="cfg3: number of requests")
     p.add_argument("--max-active", type=int, default=16, help="cfg3: simulations running at once")
     p.add_argument("--baseline-sample", type=int, default=16, help="cfg3: requests run alone for the baselines")
@@ -173,8 +177,8 @@ def census(cfg, medium: np.ndarray):
     ade = np.array([m.use_ade == 1 for m in mats])
     lossy = np.array([(m.use_ade == 0) and any(m.eps_im[q] != 0 for q in range(9)) for m in mats])
     natom = np.array([m.natom for m in mats])
-    ids, counts = np.unique(medium, return_counts=True)
-    c = dict(zip(ids.tolist(), counts.tolist()))
+    counts = np.bincount(medium.ravel(), minlength=len(mats))
+    c = {k: int(v) for k, v in enumerate(counts.tolist()) if v}
     n_ade = sum(v for k, v in c.items() if ade[k])
     n_lossy = sum(v for k, v in c.items() if lossy[k])
     atom_words = sum(v * 12 * natom[k] for k, v in c.items())
@@ -223,6 +227,7 @@ def run_ours(args, ws, rank, local, precision):
         os.chdir(old)
     holder = cfg.desc(medium, precision)
     holder.desc.device = local
+    holder.desc.z_chunk = args.z_chunk
     sim = Simulation(holder)
     nx, ny, nz = cfg.nx, cfg.ny, cfg.nz
     V = nx * ny * nz
@@ -334,6 +339,112 @@ def run_ours(args, ws, rank, local, precision):
             "h_sweep": {"achieved": round(h_gbs, 1), "frac": round(h_gbs / peak, 4), "avg_launch_ms": round(h_ms, 5),
                         "algorithmic_bytes_per_launch": hb},
             "kernel_share": {k: round(v["ms"] / max(1e-9, sum(x["ms"] for x in prof.values())), 4) for k, v in prof.items()}}}
+
+
+def run_largest(args, local):
+    """The largest single domain (1024 x 1024 x 512 cells of 8 nm, 16-cell
+    CPML, two-atom polar slab with anglex = 20 deg under a Drude-Lorentz tip,
+    z-dipole Gaussian at 1400 cm^-1, FP64 running DFT at 1370, 1400 and
+    1450 cm^-1 on the plane z = 66), FP64 and FP32: rate over --steps
+    device-timed steps, roofline of both sweeps, and the FP32 error against
+    the FP64 path on the z slice and the three DFT planes after
+    --largest-steps steps.  One context per precision, each run from step 0
+    to the same step count."""
+    import torch
+    from php_fdtd_b200 import Config, Simulation
+    from php_fdtd_b200.workloads import C_CM
+    n_total = max(args.largest_steps, args.warmup + 2 * args.steps + 40)
+    case_dir = Path(args.case_dir or tempfile.gettempdir()) / "php_bench_cfg4_largest"
+    case_dir.mkdir(parents=True, exist_ok=True)
+    t_gen = time.perf_counter()
+    make_case("cfg4", 1.0, n_total, case_dir)
+    old = os.getcwd()
+    os.chdir(case_dir)
+    try:
+        cfg = Config.load("case.cfg")
+        medium = cfg.load_medium()
+    finally:
+        os.chdir(old)
+    t_gen = time.perf_counter() - t_gen
+    V = cfg.nx * cfg.ny * cfg.nz
+    c = census(cfg, medium)
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    wn = (1370.0, 1400.0, 1450.0)
+    plane = cfg.output_slice_position + 1
+    out, state = {}, {}
+    for prec in ("fp64", "fp32"):
+        holder = cfg.desc(medium, prec)
+        holder.desc.device = local
+        t_create = time.perf_counter()
+        sim = Simulation(holder)
+        t_create = time.perf_counter() - t_create
+        pid = sim.dft_add("Ez", plane, [w * C_CM for w in wn], first_step=0, interval=1)
+        sim.probe_set(cfg.monitor_x, cfg.monitor_y, cfg.monitor_z + 1, cfg.monitor_z)
+        stream = torch.cuda.ExternalStream(sim.stream, device=torch.device("cuda", local))
+        sim.step(args.warmup)
+        sim.step(args.steps)          # records the timed region's graphs
+        sim.probe_read()
+        sim.sync()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clocks:
+            ev0.record(stream)
+            sim.step(args.steps)
+            ev1.record(stream)
+            ev1.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        sim.probe_read()
+        sim.profile(True)
+        sim.step(20)
+        prof = sim.profile_read()
+        sim.profile(False)
+        done = args.warmup + 2 * args.steps + 20
+        while done < n_total:
+            n = min(4096, n_total - done)
+            sim.step(n)
+            sim.probe_read()
+            done += n
+        sim.sync()
+        # the configuration's own z slice (position 65: plane 66, the DFT plane)
+        state[prec] = {"slice": sim.read_slice("Ez", "z", cfg.output_slice_position, f64=True),
+                       "dft": sim.dft_read(pid)[0]}
+        census_blocks = sim.block_census()
+        sim.close()
+        s = 4 if prec == "fp32" else 8
+        hb, eb = algorithmic_bytes(c, s)
+        e_ms = prof["e_sweep"]["ms"] / max(1, prof["e_sweep"]["launches"])
+        h_ms = prof["h_sweep"]["ms"] / max(1, prof["h_sweep"]["launches"])
+        out[prec] = {
+            "value": round(V * args.steps / (ms * 1e-3) / 1e9, 4), "unit": "Gcell-updates/s",
+            "ms_per_step": round(ms / args.steps, 4), "create_s": round(t_create, 2),
+            "roofline": {"bound": "hbm", "peak": peak, "unit": "GB/s",
+                         "e_sweep": {"achieved": round(eb / (e_ms * 1e-3) / 1e9, 1),
+                                     "frac": round(eb / (e_ms * 1e-3) / 1e9 / peak, 4), "avg_launch_ms": round(e_ms, 4),
+                                     "algorithmic_bytes_per_launch": eb},
+                         "h_sweep": {"achieved": round(hb / (h_ms * 1e-3) / 1e9, 1),
+                                     "frac": round(hb / (h_ms * 1e-3) / 1e9 / peak, 4), "avg_launch_ms": round(h_ms, 4),
+                                     "algorithmic_bytes_per_launch": hb}},
+            "kernel_profile": prof, "blocks": census_blocks, "clocks": clocks.summary()}
+    a, b = state["fp32"], state["fp64"]
+    err = {"steps": n_total, "reference": "FP64 GPU path (same inputs, same steps)",
+           "slice_rel_l2": float(np.linalg.norm(a["slice"] - b["slice"]) / max(np.linalg.norm(b["slice"]), 1e-300)),
+           "slice": f"Ez, z plane {plane}"}
+    for q, w in enumerate(wn):
+        f32, f64 = a["dft"][q], b["dft"][q]
+        wgt = np.abs(f64) ** 2
+        dphi = np.angle(f32 * np.conj(f64))
+        err[f"dft_{int(w)}cm-1"] = {
+            "rel_l2": float(np.linalg.norm(f32 - f64) / np.linalg.norm(f64)),
+            "amplitude_rel_l2": float(np.linalg.norm(np.abs(f32) - np.abs(f64)) / np.linalg.norm(f64)),
+            "phase_rms_rad": float(math.sqrt(np.sum(wgt * dphi ** 2) / np.sum(wgt)))}
+    return {
+        "workload": "cfg4_largest_1024x1024x512", "grid": [cfg.nx, cfg.ny, cfg.nz], "cells": V,
+        "atom_cells": c["atom_cells"], "ade_cells": c["ade_cells"], "inputs_s": round(t_gen, 1),
+        "fp64": out["fp64"], "fp32": out["fp32"],
+        "fp32_speedup_vs_fp64": round(out["fp32"]["value"] / out["fp64"]["value"], 3),
+        "error_fp32_vs_fp64": err,
+    }
 
 
 def accuracy_vs_fp64(args, local, steps: int):
@@ -616,6 +727,9 @@ def main():
         acc_steps = args.acc_steps if args.acc_steps is not None else baseline_case(WORKLOADS[args.workload]).tsteps
         if acc_steps > 0 and ws == 1:
             mixed["error_vs_fp64"] = accuracy_vs_fp64(args, local, acc_steps)
+    largest = None
+    if args.precision == "fp64" and args.workload == "cfg1" and args.scale == 1.0 and not args.no_largest:
+        largest = run_largest(args, local)
     if rank == 0:
         cpu = None
         if not args.no_cpu_baseline and ws == 1:
@@ -647,6 +761,8 @@ def main():
         }
         if mixed is not None:
             line["mixed"] = mixed
+        if largest is not None:
+            line["largest"] = largest
         print(json.dumps(line))
     barrier(ws)
     if ws > 1:

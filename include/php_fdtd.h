@@ -184,6 +184,23 @@ int php_halo_planes(php_ctx* ctx, int32_t which, void** ptrs3, uint64_t* plane_b
  * sample, after which the step counter advances.  A slab's step is
  * [E halo exchange] half 0 [H halo exchange] half 1. */
 int php_step_half(php_ctx* ctx, int32_t half);
+/* One fifth of a time step, so that a slab can hide its halo exchanges
+ * behind the planes that do not need them (the reference exchanges, then
+ * sweeps, fdtd.c:3120-3235).  Parts, enqueued on `stream` (a cudaStream_t;
+ * NULL = the context's stream):
+ *   0  H sweep of the top z chunk (reads the E halo above); first part of a
+ *      step: stages the step's source values and DFT phasors on `stream`
+ *   1  H sweep of the other chunks (no halo)
+ *   2  fused E sweep of the bottom chunk (reads the H halo below)
+ *   3  fused E sweep of the other chunks (no halo)
+ *   4  the rest of the step: ion pass, probe, DFT; the step counter advances
+ * The caller orders them on the device: 0 before 2, 3 and 4; 1 before 2 and
+ * 3 (an E chunk reads H of its own and the plane below); 2 and 3 before 4
+ * and before the next step's 0 and 1; 4 before the next step's 2 and 3.
+ * Parts 0 and 1 may run concurrently, and so may 2 and 3.  With one z chunk
+ * parts 1 and 3 launch nothing.  A step must not mix parts with
+ * php_step_half or php_step. */
+int php_step_part(php_ctx* ctx, int32_t part, void* stream);
 
 /* --- outputs -------------------------------------------------------------- */
 
@@ -298,6 +315,19 @@ int php_memory_bytes(const php_ctx* ctx, uint64_t* bytes);
 int php_estimate_bytes(const php_desc* desc, uint64_t* bytes);
 /* Number of kernel launches enqueued by the last php_step call. */
 int php_last_launch_count(const php_ctx* ctx, int32_t* launches);
+/* How the sweep kernels split the domain's blocks (a 32 x 8 tile of one z
+ * chunk) among their code paths, fixed at php_create: counts[0] fused
+ * D/E sweep blocks of one plain isotropic material on the stencil-only path,
+ * [1] such blocks with CPML or domain-edge cells, [2] blocks of the one
+ * lossy or anisotropic material whose record rides in the kernel
+ * parameters, [3] blocks of the few-atom lattice whose ions the fused sweep
+ * updates, [4] all other fused-sweep blocks (the general per-cell path),
+ * [5] H sweep blocks on the stencil-only path, [6] other H sweep blocks,
+ * [7] the total number of blocks of one sweep.  The strict mode runs every
+ * block on the general path.  No counterpart in the reference, which has
+ * one loop for every cell. */
+#define PHP_CENSUS_LEN 8
+int php_block_census(const php_ctx* ctx, int64_t* counts);
 /* Stream the context enqueues on (a cudaStream_t), for event timing. */
 int php_stream(const php_ctx* ctx, void** stream);
 

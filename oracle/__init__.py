@@ -50,10 +50,13 @@ def lib():
 
 
 def reference_binary(kind: str = "wide") -> Path:
-    """oracle/_ref/fdtd_ref{,_wide,_fast,_mp}: the reference solver itself
-    (_mp: release flags, PHP_MPI_NP ranks through the shared-memory MPI
-    stand-in of mpi_shm/mpi.h)."""
-    name = {"plain": "fdtd_ref", "wide": "fdtd_ref_wide", "fast": "fdtd_ref_fast", "mp": "fdtd_ref_mp"}[kind]
+    """oracle/_ref/fdtd_ref{,_wide,_fast,_mp,_mp_wide}: the reference solver
+    itself (_mp: release flags, PHP_MPI_NP ranks through the shared-memory
+    MPI stand-in of mpi_shm/mpi.h; _mp_wide: the same ranks with the strict
+    flags and wide outputs), or its post-processor (``post``, ``post_wide``:
+    frequency_analysis.c against the FFTW stand-in)."""
+    name = {"plain": "fdtd_ref", "wide": "fdtd_ref_wide", "fast": "fdtd_ref_fast", "mp": "fdtd_ref_mp",
+            "mp_wide": "fdtd_ref_mp_wide", "post": "frequency_analysis", "post_wide": "frequency_analysis_wide"}[kind]
     return HERE / "_ref" / name
 
 

@@ -135,6 +135,7 @@ DEVICE_SYMBOLS = {
     "php_dft_read": (_i, [C.c_void_p, _i, _dp, C.POINTER(_i)]),
     "php_memory_bytes": (_i, [C.c_void_p, C.POINTER(C.c_uint64)]),
     "php_last_launch_count": (_i, [C.c_void_p, C.POINTER(_i)]),
+    "php_block_census": (_i, [C.c_void_p, C.POINTER(C.c_int64)]),
     "php_stream": (_i, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "php_profile_enable": (_i, [C.c_void_p, _i]),
     "php_profile_read": (_i, [C.c_void_p, _dp, C.POINTER(C.c_int64)]),
@@ -142,6 +143,7 @@ DEVICE_SYMBOLS = {
     "php_create_slab": (_i, [C.POINTER(Desc), _i, _i, C.POINTER(C.c_void_p)]),
     "php_halo_planes": (_i, [C.c_void_p, _i, C.POINTER(C.c_void_p), C.POINTER(C.c_uint64)]),
     "php_step_half": (_i, [C.c_void_p, _i]),
+    "php_step_part": (_i, [C.c_void_p, _i, C.c_void_p]),
     "php_prepare": (_i, [C.c_void_p, _i]),
     "php_server_create": (_i, [C.POINTER(ServerDesc), C.POINTER(C.c_void_p)]),
     "php_server_destroy": (_i, [C.c_void_p]),

@@ -61,7 +61,9 @@ struct php_ctx {
     int n3max = 0, namax_tpl = 0;
     int64_t nslot = 0;           /* pool slots, padded to a multiple of 32 */
     int z_off = 0, nz_glob = 0;  /* z slab: global index of local plane 0, global nz */
-    int step_part = 3;           /* launches of a step: 1 H sweep, 2 the rest, 3 both */
+    int step_part = 7;           /* launches of a step: 1 H sweep, 2 fused E sweep, 4 the rest (ions, probe, DFT) */
+    int zc_first = 0, zc_count = -1; /* z chunks the sweeps launch over (-1: all) */
+    bool part_staged = false;    /* php_step_part: this step's inputs are on the device */
     int num_sms = 148;
     bool any_ade = false, any_atoms = false;
     cudaStream_t stream = nullptr;
@@ -140,6 +142,7 @@ struct php_ctx {
 
     /* TMA maps of the sweep kernels */
     TmaMaps maps;
+    int64_t census[PHP_CENSUS_LEN] = {}; /* php_block_census */
     int32_t* err_flag = nullptr;
 
     /* per-kernel timing (php_profile_enable) */
@@ -662,19 +665,25 @@ static void launch_step_t(php_ctx* ctx, int s_local, int& launches)
 {
     StepArgs<R> a = make_args<R>(ctx, s_local);
     dim3 block(kBlockX, kBlockY, 1);
-    dim3 grid((ctx->nx + kBlockX - 1) / kBlockX, (ctx->ny + kBlockY - 1) / kBlockY, (ctx->nz + ctx->zchunk - 1) / ctx->zchunk);
-    const bool do_h = ctx->step_part & 1, do_e = ctx->step_part & 2;
-    if (do_h) {
+    const int nchunk = (ctx->nz + ctx->zchunk - 1) / ctx->zchunk;
+    a.zc0 = ctx->zc_count < 0 ? 0 : ctx->zc_first;
+    dim3 grid((ctx->nx + kBlockX - 1) / kBlockX, (ctx->ny + kBlockY - 1) / kBlockY,
+              ctx->zc_count < 0 ? nchunk : ctx->zc_count);
+    const bool do_h = ctx->step_part & 1, do_e = ctx->step_part & 2, do_rest = ctx->step_part & 4;
+    if (grid.z == 0) { /* an empty part: no sweep blocks */
+    } else if (do_h) {
         prof_mark(ctx, s_local, 0, 0);
         h_sweep_tma<R, STRICT><<<grid, block, TmaGeom<R>::H_SMEM, ctx->stream>>>(a, ctx->maps);
         prof_mark(ctx, s_local, 0, 1);
         launches++;
     }
-    if (!do_e) return;
-    prof_mark(ctx, s_local, 1, 0);
-    e_sweep_tma<R, STRICT, NA><<<grid, block, TmaGeom<R>::E_SMEM + a.nmat * sizeof(MatCoef<R>), ctx->stream>>>(a, ctx->maps);
-    prof_mark(ctx, s_local, 1, 1);
-    launches++;
+    if (do_e && grid.z > 0) {
+        prof_mark(ctx, s_local, 1, 0);
+        e_sweep_tma<R, STRICT, NA><<<grid, block, TmaGeom<R>::E_SMEM + a.nmat * sizeof(MatCoef<R>), ctx->stream>>>(a, ctx->maps);
+        prof_mark(ctx, s_local, 1, 1);
+        launches++;
+    }
+    if (!do_rest) return;
     if constexpr (!STRICT && NA == 0) {
         if (ctx->ion_split) {
             prof_mark(ctx, s_local, 4, 0);
@@ -1386,6 +1395,13 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
                     pm[b] = (uint8_t)kPlainTensor;
                     nplain++;
                 }
+        for (size_t b = 0; b < pm.size(); b++) {
+            const int c = pm[b] == 255 ? 4 : pm[b] == kPlainAtoms ? 3 : pm[b] == kPlainTensor ? 2
+                        : pm[b] >= kPlainCpml ? 1 : 0;
+            ctx->census[c]++;
+            ctx->census[ph[b] ? 5 : 6]++;
+        }
+        ctx->census[7] = (int64_t)pm.size();
         if (nplain) {
             if ((rc = dalloc(ctx, (void**)&ctx->plain_blk, pm.size()))) return rc;
             if ((rc = upload(ctx, ctx->plain_blk, pm.data(), pm.size()))) return rc;
@@ -1680,9 +1696,9 @@ int php_step_half(php_ctx* ctx, int32_t half)
         if (rc) return rc;
     }
     ctx->step_in = ctx->step_in_dev[b];
-    ctx->step_part = half == 0 ? 1 : 2;
+    ctx->step_part = half == 0 ? 1 : 6;
     pick_step(ctx).launch(ctx, 0, launches);
-    ctx->step_part = 3;
+    ctx->step_part = 7;
     CK(cudaGetLastError());
     if (half == 1) {
         ctx->chunk_no++;
@@ -1690,6 +1706,47 @@ int php_step_half(php_ctx* ctx, int32_t half)
     }
     ctx->last_launches = launches;
     return PHP_OK;
+}
+
+int php_step_part(php_ctx* ctx, int32_t part, void* stream)
+{
+    if (!ctx || part < 0 || part > 4) return PHP_ERR_INPUT;
+    ctx->last_launches = 0;
+    int launches = 0;
+    const int b = ctx->chunk_no & 1;
+    const int nchunk = (ctx->nz + ctx->zchunk - 1) / ctx->zchunk;
+    cudaStream_t own = ctx->stream;
+    if (stream) ctx->stream = static_cast<cudaStream_t>(stream);
+    int rc = PHP_OK;
+    if (part == 0 && !ctx->part_staged) { /* the step's source values and DFT phasors */
+        rc = stage_step_inputs(ctx, 1, b);
+        ctx->part_staged = rc == PHP_OK;
+    }
+    if (rc == PHP_OK && part != 0 && !ctx->part_staged)
+        rc = fail(ctx, PHP_ERR_STATE, "php_step_part %d before part 0 of the step", part);
+    if (rc == PHP_OK) {
+        ctx->step_in = ctx->step_in_dev[b];
+        /* H: part 0 the top chunk, part 1 the others; E: part 2 the bottom
+         * chunk, part 3 the others; part 4 the rest of the step */
+        static const int kPartBits[5] = {1, 1, 2, 2, 4};
+        ctx->step_part = kPartBits[part];
+        ctx->zc_first = part == 0 ? nchunk - 1 : part == 3 ? 1 : 0;
+        ctx->zc_count = part == 0 || part == 2 ? 1 : part == 4 ? 0 : nchunk - 1;
+        pick_step(ctx).launch(ctx, 0, launches);
+        ctx->step_part = 7;
+        ctx->zc_first = 0;
+        ctx->zc_count = -1;
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) rc = fail(ctx, PHP_ERR_CUDA, "%s", cudaGetErrorString(e));
+    }
+    ctx->stream = own;
+    if (rc == PHP_OK && part == 4) {
+        ctx->part_staged = false;
+        ctx->chunk_no++;
+        ctx->t++;
+    }
+    ctx->last_launches = launches;
+    return rc;
 }
 
 int php_destroy(php_ctx* ctx)
@@ -2225,6 +2282,13 @@ int php_last_launch_count(const php_ctx* ctx, int32_t* launches)
 {
     if (!ctx || !launches) return PHP_ERR_INPUT;
     *launches = ctx->last_launches;
+    return PHP_OK;
+}
+
+int php_block_census(const php_ctx* ctx, int64_t* counts)
+{
+    if (!ctx || !counts) return PHP_ERR_INPUT;
+    for (int q = 0; q < PHP_CENSUS_LEN; q++) counts[q] = ctx->census[q];
     return PHP_OK;
 }
 

@@ -144,6 +144,7 @@ struct StepArgs {
     int64_t nslot;
     int32_t nmat;
     int32_t nx, ny, nz, nxp, L, zchunk;
+    int32_t zc0;                /* first z chunk of the launch (blockIdx.z + zc0 is the chunk) */
     int64_t plane;             /* nxp * ny */
     /* strict scalars */
     double dt, dxs, dys, dzs, mu0, eps0, c1, e0dt2;

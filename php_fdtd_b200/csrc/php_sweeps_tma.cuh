@@ -194,7 +194,8 @@ __global__ void __launch_bounds__(kBlockX * kBlockY) h_sweep_tma(const __grid_co
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * G::TX + tx;
     const int i0 = blockIdx.x * G::TX, j0 = blockIdx.y * G::TY;
     const int i = i0 + tx, j = j0 + ty;
-    const int k0 = blockIdx.z * a.zchunk;
+    const int bz = blockIdx.z + a.zc0;
+    const int k0 = bz * a.zchunk;
     const int k1 = min(k0 + a.zchunk, a.nz);
     if (k0 >= k1) return; /* uniform over the block */
 
@@ -225,7 +226,7 @@ __global__ void __launch_bounds__(kBlockX * kBlockY) h_sweep_tma(const __grid_co
     /* a plain block (no CPML cell, every cell updated; marked on the host):
      * the stencil with the kappa = 1 factors only, the same arithmetic as the
      * general path below takes for such cells */
-    if (!STRICT && a.plain_h && a.plain_h[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x]) {
+    if (!STRICT && a.plain_h && a.plain_h[((size_t)bz * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x]) {
         const R khx = a.khp[0], khy = a.khp[1], khz = a.khp[2];
         for (int k = k0; k < k1; ++k) {
             bool ok = true;
@@ -424,7 +425,8 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * G::TX + tx;
     const int i0 = blockIdx.x * G::TX, j0 = blockIdx.y * G::TY;
     const int i = i0 + tx, j = j0 + ty;
-    const int k0 = blockIdx.z * a.zchunk;
+    const int bz = blockIdx.z + a.zc0;
+    const int k0 = bz * a.zchunk;
     const int k1 = min(k0 + a.zchunk, a.nz);
     if (k0 >= k1) return; /* uniform over the block */
 
@@ -466,7 +468,7 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
      * cell; marked on the host): D += curl H with the kappa = 1 factors and
      * E = iso D, nothing per cell beyond the stencil (the same arithmetic as
      * the general path below takes for such cells) */
-    const int pm = (!STRICT && a.plain_blk) ? a.plain_blk[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x]
+    const int pm = (!STRICT && a.plain_blk) ? a.plain_blk[((size_t)bz * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x]
                                             : 255;
     if constexpr (NAMAX > 0 && NAMAX <= 4) {
         if (pm == kPlainAtoms) {

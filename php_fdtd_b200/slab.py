@@ -1,17 +1,22 @@
 """z-slab decomposition of one domain over several GPUs.
 
 The reference splits z across MPI ranks (fdtd.c:2761-2771) and exchanges the
-boundary planes each half step (fdtd.c:3120, 3235).  Here a slab is a
-device context for its planes (php_create_slab); per time step each slab
+boundary planes each half step (fdtd.c:3120, 3235): E plane 0 goes down
+before the H sweep, H plane nz-1 goes up before the D/E sweep.  Here a slab
+is a device context for its planes (php_create_slab), and each time step
+runs in the parts of php_step_part so that the exchanges hide behind the
+planes that do not need them:
 
-    sends E plane 0 down, receives E into its halo plane nz  (exchange_e)
-    runs the H sweep                                        (half 0)
-    sends H plane nz-1 up, receives H into its halo plane -1 (exchange_h)
-    runs the D/E sweep, ion pass, probe and DFT             (half 1)
+    side stream   H sweep, lower chunks (1)      E sweep, upper chunks (3)
+    main stream   H sweep, top chunk (0)  -> H plane up / H halo from below
+                  E sweep, bottom chunk (2) -> E plane 0 down / E halo from above
+                  ion pass, probe, DFT (4)
 
-Only plane data crosses between GPUs: three planes per neighbour and half
-step, device to device (NCCL send/receive between processes, or copies
-between the slabs of one process).  No collective is on the data path.
+Only plane data crosses between slabs: three planes per neighbour and
+exchange (NCCL send/receive between processes, page-locked host staging
+over any torch.distributed backend, or device copies between the slabs of
+one process).  No collective is on the data path, and nothing waits on the
+host between the parts of a step except the host-staged transport.
 """
 from __future__ import annotations
 
@@ -98,13 +103,27 @@ class Slab(Simulation):
     def half(self, h: int):
         self._ck(self._lib.php_step_half(self._ctx, int(h)))
 
+    def part(self, p: int, stream: int = 0):
+        """php_step_part on a cudaStream_t handle (0 = the slab's stream)."""
+        self._ck(self._lib.php_step_part(self._ctx, int(p), C.c_void_p(stream or None)))
+
+
+class _StepEvents:
+    """The events that order one slab's parts across its two streams."""
+
+    def __init__(self):
+        import torch
+        self.h0, self.h1, self.e3, self.p4 = (torch.cuda.Event() for _ in range(4))
+
 
 class LocalSlabs:
     """All slabs of a domain in one process (on one GPU, or one per GPU of
-    the process): the halo planes are copied device to device between the
-    halves of every step, in slab order."""
+    the process): the halo planes are copied device to device, and every
+    dependency between parts, copies and slabs is a CUDA event, so a step is
+    enqueued without any host synchronisation."""
 
     def __init__(self, holder: DescHolder, nslabs: int, devices: Sequence[int] = (0,)):
+        import torch
         self.ranges = slab_ranges(holder.desc.nz, nslabs)
         self.slabs = []
         for r, (z0, n) in enumerate(self.ranges):
@@ -112,61 +131,194 @@ class LocalSlabs:
             h.desc.device = devices[r % len(devices)]
             self.slabs.append(Slab(h, z0, n))
         self._p = [{w: s.planes(w) for w in range(4)} for s in self.slabs]
+        self._main, self._side, self._ev = [], [], []
+        for s in self.slabs:
+            dev = torch.device("cuda", s.holder.desc.device)
+            self._main.append(torch.cuda.ExternalStream(s.stream, device=dev))
+            self._side.append(torch.cuda.Stream(device=dev))
+            self._ev.append(_StepEvents())
+        n = len(self.slabs)
+        self._e2 = [torch.cuda.Event() for _ in range(n)]     # E bottom chunk done (slab r)
+        self._cp_e = [torch.cuda.Event() for _ in range(n)]   # E plane 0 of r+1 copied into r
+        self._cp_h = [torch.cuda.Event() for _ in range(n)]   # H top plane of r-1 copied into r
+        self._copy_e()
 
-    def _copy(self, dst, src):
+    @staticmethod
+    def _copy(dst, src):
         for d, s in zip(dst, src):
-            d.copy_(s)
+            d.copy_(s, non_blocking=True)
+
+    def _copy_e(self):
+        """E plane 0 of slab r+1 into the halo above slab r, on r's main
+        stream once r+1's bottom E chunk is done."""
+        import torch
+        for r in range(len(self.slabs) - 1):
+            m = self._main[r]
+            m.wait_event(self._e2[r + 1])
+            with torch.cuda.stream(m):
+                self._copy(self._p[r][1], self._p[r + 1][0])
+            self._cp_e[r].record(m)
 
     def step(self, n: int = 1):
         import torch
-        S = self.slabs
+        S, M, Sd, EV = self.slabs, self._main, self._side, self._ev
+        R = len(S)
         for _ in range(n):
-            for s in S:
-                s.sync()
-            for r in range(len(S) - 1):           # E plane 0 of r+1 -> halo above r
-                self._copy(self._p[r][1], self._p[r + 1][0])
-            torch.cuda.synchronize()
-            for s in S:
-                s.half(0)
-            for s in S:
-                s.sync()
-            for r in range(1, len(S)):            # H top plane of r-1 -> halo below r
-                self._copy(self._p[r][3], self._p[r - 1][2])
-            torch.cuda.synchronize()
-            for s in S:
-                s.half(1)
-        for s in S:
+            for r in range(R):                      # H sweep, chunks below the top (no halo)
+                Sd[r].wait_event(EV[r].p4)
+                S[r].part(1, Sd[r].cuda_stream)
+                EV[r].h1.record(Sd[r])
+            for r in range(R):                      # H sweep, top chunk (E halo above)
+                if r + 1 < R:
+                    M[r].wait_event(self._cp_h[r + 1])   # the last copy of this H plane is done
+                S[r].part(0, M[r].cuda_stream)
+                EV[r].h0.record(M[r])
+            for r in range(R):                      # E sweep, chunks above the bottom (no halo)
+                Sd[r].wait_event(EV[r].h0)
+                S[r].part(3, Sd[r].cuda_stream)
+                EV[r].e3.record(Sd[r])
+            for r in range(1, R):                   # H plane nz-1 of r-1 -> halo below r
+                M[r].wait_event(EV[r - 1].h0)
+                with torch.cuda.stream(M[r]):
+                    self._copy(self._p[r][3], self._p[r - 1][2])
+                self._cp_h[r].record(M[r])
+            for r in range(R):                      # E sweep, bottom chunk (H halo below)
+                M[r].wait_event(EV[r].h1)
+                if r > 0:
+                    M[r].wait_event(self._cp_e[r - 1])   # E plane 0 copied before it is rewritten
+                S[r].part(2, M[r].cuda_stream)
+                self._e2[r].record(M[r])
+            self._copy_e()                          # E halos of the next step
+            for r in range(R):                      # ion pass, probe, DFT
+                M[r].wait_event(EV[r].e3)
+                S[r].part(4, M[r].cuda_stream)
+                EV[r].p4.record(M[r])
+
+    def sync(self):
+        for s in self.slabs:
             s.sync()
 
     def read_volume(self, comp) -> np.ndarray:
+        self.sync()
         return np.concatenate([s.read_volume(comp) for s in self.slabs], axis=2)
 
     def close(self):
+        self.sync()
         for s in self.slabs:
             s.close()
 
 
+class DeviceTransport:
+    """Plane exchange of device tensors with torch.distributed point to
+    point (NCCL between GPUs), ordered on the current stream."""
+
+    def __init__(self, dist):
+        self.dist = dist
+
+    def exchange(self, sends, recvs, stream):
+        import torch
+        ops = [self.dist.P2POp(self.dist.isend, t, peer) for peer, ts in sends for t in ts]
+        ops += [self.dist.P2POp(self.dist.irecv, t, peer) for peer, ts in recvs for t in ts]
+        if not ops:
+            return
+        with torch.cuda.stream(stream):
+            for w in self.dist.batch_isend_irecv(ops):
+                w.wait()
+
+
+class HostTransport:
+    """Plane exchange through page-locked host buffers over any
+    torch.distributed backend (gloo included): the device copies run on the
+    slab's stream, and the host waits for the copy out before it sends.
+    For GPUs without a peer path, and for CPU-side tests of the schedule."""
+
+    def __init__(self, dist):
+        self.dist = dist
+        self._buf = {}
+
+    def _host(self, key, t):
+        import torch
+        b = self._buf.get(key)
+        if b is None:
+            b = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+            self._buf[key] = b
+        return b
+
+    def exchange(self, sends, recvs, stream):
+        import torch
+        out = [(peer, [self._host(("s", peer, q), t) for q, t in enumerate(ts)]) for peer, ts in sends]
+        inn = [(peer, [self._host(("r", peer, q), t) for q, t in enumerate(ts)]) for peer, ts in recvs]
+        with torch.cuda.stream(stream):
+            for (_, ts), (_, hs) in zip(sends, out):
+                for t, h in zip(ts, hs):
+                    h.copy_(t, non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record(stream)
+        ev.synchronize()
+        works = [self.dist.isend(h, peer) for peer, hs in out for h in hs]
+        works += [self.dist.irecv(h, peer) for peer, hs in inn for h in hs]
+        for w in works:
+            w.wait()
+        with torch.cuda.stream(stream):
+            for (_, ts), (_, hs) in zip(recvs, inn):
+                for t, h in zip(ts, hs):
+                    t.copy_(h, non_blocking=True)
+
+
 class DistSlab:
     """This rank's slab of a domain decomposed over torch.distributed ranks
-    (one process per GPU, NCCL between neighbours)."""
+    (one process per GPU).  transport: "device" (NCCL point to point on
+    device tensors) or "host" (page-locked host staging, any backend)."""
 
-    def __init__(self, holder: DescHolder, rank: int, size: int):
+    def __init__(self, holder: DescHolder, rank: int, size: int, transport: str = "device"):
+        import torch
         import torch.distributed as dist
         self.dist = dist
         self.rank, self.size = rank, size
         self.z0, n = slab_ranges(holder.desc.nz, size)[rank]
         self.slab = Slab(holder, self.z0, n)
         self._p = {w: self.slab.planes(w) for w in range(4)}
+        dev = torch.device("cuda", holder.desc.device)
+        self._main = torch.cuda.ExternalStream(self.slab.stream, device=dev)
+        self._side = torch.cuda.Stream(device=dev)
+        self._ev = _StepEvents()
+        self.transport = HostTransport(dist) if transport == "host" else DeviceTransport(dist)
+        self._exchange_e()
+
+    def _exchange_e(self):
+        """E plane 0 to rank-1; the halo above from rank+1."""
+        r, n = self.rank, self.size
+        self.transport.exchange([(r - 1, self._p[0])] if r > 0 else [],
+                                [(r + 1, self._p[1])] if r < n - 1 else [], self._main)
+
+    def _exchange_h(self):
+        """H plane nz-1 to rank+1; the halo below from rank-1."""
+        r, n = self.rank, self.size
+        self.transport.exchange([(r + 1, self._p[2])] if r < n - 1 else [],
+                                [(r - 1, self._p[3])] if r > 0 else [], self._main)
 
     def step(self, n: int = 1):
-        import torch
-        stream = torch.cuda.ExternalStream(self.slab.stream, device=self._p[0][0].device)
-        with torch.cuda.stream(stream):
-            for _ in range(n):
-                exchange_e(self.rank, self.size, self._p[0], self._p[1], self.dist)
-                self.slab.half(0)
-                exchange_h(self.rank, self.size, self._p[2], self._p[3], self.dist)
-                self.slab.half(1)
+        S, M, Sd, ev = self.slab, self._main, self._side, self._ev
+        for _ in range(n):
+            Sd.wait_event(ev.p4)
+            S.part(1, Sd.cuda_stream)       # H sweep below the top chunk
+            ev.h1.record(Sd)
+            S.part(0, M.cuda_stream)        # H sweep, top chunk (E halo received)
+            ev.h0.record(M)
+            Sd.wait_event(ev.h0)
+            S.part(3, Sd.cuda_stream)       # E sweep above the bottom chunk, behind both exchanges
+            ev.e3.record(Sd)
+            self._exchange_h()
+            M.wait_event(ev.h1)
+            S.part(2, M.cuda_stream)        # E sweep, bottom chunk (H halo received)
+            self._exchange_e()              # E halo of the next step
+            M.wait_event(ev.e3)
+            S.part(4, M.cuda_stream)        # ion pass, probe, DFT
+            ev.p4.record(M)
+
+    def sync(self):
+        self.slab.sync()
 
     def close(self):
+        self.slab.sync()
         self.slab.close()

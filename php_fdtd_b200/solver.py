@@ -387,6 +387,14 @@ class Simulation:
         self._ck(self._lib.php_last_launch_count(self._ctx, C.byref(v)))
         return v.value
 
+    CENSUS_KEYS = ("e_plain", "e_plain_cpml", "e_tensor", "e_atoms", "e_general", "h_plain", "h_general", "blocks")
+
+    def block_census(self) -> dict:
+        """Blocks per sweep code path (php_block_census)."""
+        n = (C.c_int64 * 8)()
+        self._ck(self._lib.php_block_census(self._ctx, n))
+        return {k: int(n[q]) for q, k in enumerate(self.CENSUS_KEYS)}
+
     def profile(self, enable: bool = True):
         """Per-kernel device timing of the following steps (php_profile_enable)."""
         self._ck(self._lib.php_profile_enable(self._ctx, int(bool(enable))))

@@ -122,7 +122,7 @@ def write_medium(path: Path, medium: np.ndarray):
     nx, ny, nz = medium.shape
     with open(path, "wb") as f:
         f.write(struct.pack("iii", nx, ny, nz))
-        f.write(medium.tobytes())
+        medium.tofile(f)
 
 
 # ------------------------------------------------------------------- cases
@@ -301,31 +301,83 @@ _add(CaseSpec("multi_source_ragged", 21, 11, 9, 40, pml=2, output_component="Ey"
 _add(CaseSpec("no_pml_tiny", 3, 3, 2, 12, pml=0, output_interval=3, output_component="Ex", slice_axis="y", slice_pos=1,
               sources=[_dip(1, 1, 0, c="x", wn=1200, t0=1e-16, tau=0.5e-16)], materials=[MAT_ANISO],
               medium_fn=_blocks((0, 2, 0, 2, 0, 0, 4)), monitor="x=1,y=1,z=0,atom=0,dir=x"))
+# a sine-driven run with an explicit dt and 101 z slices above a two-atom
+# slab: the input of the reference's post-processor (frequency_analysis.c),
+# whose spectra pin the running DFT
+_add(CaseSpec("spectra_dft", 24, 22, 20, 201, pml=4, output_interval=2, output_component="Ez", slice_axis="z",
+              slice_pos=9, dt=10e-9 / (299792458.0 * math.sqrt(3.0)) * 0.99,
+              sources=["type=sinusoidal, x=12,y=11,z=13, amplitude=1.0, frequency=1.2e15, component=z"],
+              materials=[MAT_IONS2, MAT_ANISO], medium_fn=_blocks((0, 23, 0, 21, 0, 3, 8), (6, 17, 5, 16, 4, 5, 4)),
+              files_fn=_all_files, monitor="x=12,y=11,z=2,atom=0,dir=z"))
+
+
+MAT_GLASS = "id=12, name=glass, eps_xx=2.25, eps_yy=2.25, eps_zz=2.25"
+
+
+def blocks_mixed_case(tsteps: int = 100) -> CaseSpec:
+    """A 96 x 64 x 64 grid in which every block class of the device sweeps
+    occurs: a two-atom polar slab (z < 16) whose tiles hold the lattice alone,
+    a lossy rotated anisotropic layer (16 <= z < 24) filling whole tiles,
+    vacuum interior tiles and vacuum tiles in the CPML or on the domain edge,
+    whole tiles of an isotropic dielectric, and mixed tiles: a Drude metal
+    block (ADE) cutting through tiles, a rotated two-atom inclusion in the
+    slab, and the tile of the source."""
+    def medium(nx, ny, nz):
+        m = np.zeros((nx, ny, nz), np.int32)
+        m[:, :, :16] = 8
+        m[:, :, 16:24] = 5
+        m[20:44, 20:28, 2:6] = 9          # rotated lattice inside the slab
+        m[32:64, 16:32, 30:34] = 12       # whole 32 x 8 tiles of glass
+        m[40:56, 36:44, 26:40] = 7        # ADE metal, partial tiles
+        return m
+    return CaseSpec("blocks_mixed", 96, 64, 64, tsteps, pml=6, output_interval=10, output_component="Ez",
+                    slice_axis="z", slice_pos=22,
+                    sources=[_dip(48, 32, 50, wn=1370, t0=3e-16, tau=1e-16),
+                             "type=sinusoidal, x=70,y=40,z=28, amplitude=0.5, frequency=3.0e13, component=x"],
+                    materials=[MAT_IONS2, MAT_IONS2_ROT, MAT_LOSSY_ROTZ, MAT_METAL, MAT_GLASS], medium_fn=medium,
+                    files_fn=_all_files, monitor="x=48,y=32,z=12,atom=1,dir=z")
 
 
 # -------------------------------------------------------- benchmark configs
 
 
-def cone_tip_mask(nx, ny, nz, dx, dz, apex_xy, apex_k, radius_m, half_angle_deg, top_k=None):
+def cone_tip_box(nx, ny, nz, dx, dz, apex_xy, apex_k, radius_m, half_angle_deg, top_k=None):
     """Cone along +z with a spherical cap at its apex (apex cell apex_k):
-    cells whose centre is inside the cap sphere or the cone above it."""
-    i = np.arange(nx)[:, None, None]
-    j = np.arange(ny)[None, :, None]
-    k = np.arange(nz)[None, None, :]
-    x = (i - apex_xy[0]) * dx
-    y = (j - apex_xy[1]) * dx
-    z = (k - apex_k) * dz
+    cells whose centre is inside the cap sphere or the cone above it.
+    Returns (box, mask): the index box (three slices) holding every such
+    cell and the mask over that box, so large grids are painted without
+    whole-grid temporaries."""
     a = math.radians(half_angle_deg)
     # sphere tangent to the cone, touching z = 0 at the apex
     zc = radius_m
     zt = zc - radius_m * math.sin(a)  # height where cone and sphere meet
+    k_top = nz - 1 if top_k is None else min(nz - 1, top_k)
+    k0 = max(0, apex_k)                # sphere and cone lie at z >= 0
+    z_max = (k_top - apex_k) * dz
+    rho_max = max(radius_m, radius_m * math.cos(a) + max(0.0, z_max - zt) * math.tan(a))
+    reach = int(math.ceil(rho_max / dx)) + 1
+    i0, i1 = max(0, apex_xy[0] - reach), min(nx, apex_xy[0] + reach + 1)
+    j0, j1 = max(0, apex_xy[1] - reach), min(ny, apex_xy[1] + reach + 1)
+    k1 = k_top + 1
+    box = (slice(i0, max(i0, i1)), slice(j0, max(j0, j1)), slice(k0, max(k0, k1)))
+    i = np.arange(box[0].start, box[0].stop)[:, None, None]
+    j = np.arange(box[1].start, box[1].stop)[None, :, None]
+    k = np.arange(box[2].start, box[2].stop)[None, None, :]
+    x = (i - apex_xy[0]) * dx
+    y = (j - apex_xy[1]) * dx
+    z = (k - apex_k) * dz
     rho = np.sqrt(x * x + y * y)
     in_sphere = (x * x + y * y + (z - zc) ** 2) <= radius_m ** 2
     r_cone = radius_m * math.cos(a) + (z - zt) * math.tan(a)
     in_cone = (z >= zt) & (rho <= r_cone)
-    m = in_sphere | in_cone
-    if top_k is not None:
-        m &= k <= top_k
+    return box, in_sphere | in_cone
+
+
+def cone_tip_mask(nx, ny, nz, dx, dz, apex_xy, apex_k, radius_m, half_angle_deg, top_k=None):
+    """The cone tip of cone_tip_box as a mask over the whole grid."""
+    m = np.zeros((nx, ny, nz), bool)
+    box, sub = cone_tip_box(nx, ny, nz, dx, dz, apex_xy, apex_k, radius_m, half_angle_deg, top_k)
+    m[box] = sub
     return m
 
 
@@ -417,8 +469,9 @@ def baseline_case(idx: int, tsteps: Optional[int] = None, seed: int = 0, scale: 
         def medium(nx_, ny_, nz_):
             m = np.zeros((nx_, ny_, nz_), np.int32)
             m[:, :, :slab] = 4
-            m[cone_tip_mask(nx_, ny_, nz_, dl, dl, (nx_ // 2, ny_ // 2), slab + 2, 20e-9, 15.0,
-                            top_k=nz_ - max(2, int(16 * scale)) - 2)] = 5
+            box, sub = cone_tip_box(nx_, ny_, nz_, dl, dl, (nx_ // 2, ny_ // 2), slab + 2, 20e-9, 15.0,
+                                    top_k=nz_ - max(2, int(16 * scale)) - 2)
+            m[box][sub] = 5
             return m
         return CaseSpec(
             "cfg4_largest_1024x1024x512", nx, nx, nz, tsteps or 20000, delta=(dl, dl, dl), pml=max(2, int(16 * scale)),
@@ -432,6 +485,23 @@ def baseline_case(idx: int, tsteps: Optional[int] = None, seed: int = 0, scale: 
                                              np.stack([np.diag([2.7, 2.7, 0.9]), -np.diag([2.7, 2.7, 0.9])]))),
             monitor=f"x={nx // 2},y={nx // 2},z={slab + 1},atom=0,dir=z")
     raise ValueError(f"no single-domain workload {idx}")
+
+
+# parity cases at the benchmark workloads' own sizes: the full-length
+# config 0, 200-step truncations of configs 1 and 2, and the block-class mix
+PARITY_BASELINE_CASES = ("cfg0_full", "cfg1_200", "cfg2_200", "blocks_mixed")
+
+
+def parity_baseline_case(name: str) -> CaseSpec:
+    if name == "cfg0_full":
+        return baseline_case(0)
+    if name == "cfg1_200":
+        return baseline_case(1, tsteps=200)
+    if name == "cfg2_200":
+        return baseline_case(2, tsteps=200)
+    if name == "blocks_mixed":
+        return blocks_mixed_case()
+    raise ValueError(f"no baseline parity case {name}")
 
 
 # ------------------------------------------------------ serving requests

@@ -68,14 +68,17 @@ def clean_outputs(case_dir: Path):
             p.unlink()
 
 
-def run_reference(case_dir: Path, kind: str = "wide", timeout: int = 600) -> dict:
+def run_reference(case_dir: Path, kind: str = "wide", timeout: int = 600, ranks: int = 1) -> dict:
+    """kind: plain / wide / fast (one rank), mp / mp_wide (``ranks`` ranks
+    through the shared-memory MPI stand-in)."""
     from oracle import reference_binary
     exe = reference_binary(kind)
     if not exe.exists():
         raise FileNotFoundError(exe)
     clean_outputs(case_dir)
-    p = subprocess.run([str(exe), "case.cfg"], cwd=case_dir, capture_output=True, text=True, timeout=timeout)
-    res = collect_files(case_dir, wide=(kind == "wide"))
+    env = dict(os.environ, PHP_MPI_NP=str(ranks))
+    p = subprocess.run([str(exe), "case.cfg"], cwd=case_dir, capture_output=True, text=True, timeout=timeout, env=env)
+    res = collect_files(case_dir, wide=kind in ("wide", "mp_wide"))
     res["returncode"] = p.returncode
     res["stdout"] = p.stdout
     return res

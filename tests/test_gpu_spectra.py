@@ -1,45 +1,81 @@
-"""Near-field spectra (fdtd_b200 --spectra): the frequency_slice_*.txt files
-the solver writes from its running DFT, against the reference's
-post-processor restated with NumPy's FFT over the slice files of the same
-run (oracle/spectra.py)."""
-import math
+"""Near-field spectra and the running DFT against the reference's own
+post-processor (frequency_analysis.c, compiled unmodified against the FFTW
+stand-in of oracle/fftw_stub), run on the reference's own slices of the
+spectra_dft golden case (tests/golden/make_golden.py):
+
+  - fdtd_b200 --spectra writes frequency_slice_*.txt from its running DFT;
+    the files must match the post-processor's (golden post/) header for
+    header and row for row, values within the %.6e text precision;
+  - the running-DFT accumulators (php_dft_read, FP64 samples, no float32
+    cast) over N samples, divided by N, must equal the post-processor's
+    values on the reference's float64 slices (golden spectra.npz, printed
+    %.17e) to relative L2 <= 1e-10, real and imaginary parts (amplitude and
+    phase).
+"""
 import subprocess
 from pathlib import Path
 
 import numpy as np
 import pytest
 
+import harness as H
 from oracle import spectra
-from php_fdtd_b200.workloads import CaseSpec, write_case
+from php_fdtd_b200 import Config, Simulation
 
 pytestmark = pytest.mark.gpu
 EXE = Path(__file__).resolve().parents[1] / "php_fdtd_b200" / "fdtd_b200"
+CASE = "spectra_dft"
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_spectra_match_the_post_processor(precision, tmp_path):
-    dl = 10e-9
-    dt = dl / (299792458.0 * math.sqrt(3.0)) * 0.99
-    spec = CaseSpec("spectra", 24, 22, 20, 201, delta=(dl, dl, dl), pml=4, output_interval=2,
-                    output_component="Ez", slice_axis="z", slice_pos=9, dt=dt,
-                    sources=["type=sinusoidal, x=12,y=11,z=13, amplitude=1.0, frequency=1.2e15, component=z"],
-                    materials=["id=4, name=slab, eps_xx=4.0, eps_yy=4.0, eps_zz=3.0"],
-                    medium_fn=lambda nx, ny, nz: np.pad(np.full((nx, ny, 4), 4, np.int32), ((0, 0), (0, 0), (0, nz - 4))))
-    write_case(spec, tmp_path)
-    r = subprocess.run([str(EXE), "case.cfg", precision, "--spectra"], cwd=tmp_path, capture_output=True, text=True,
+@pytest.mark.parametrize("precision,tol", [("fp64-strict", 2e-6), ("fp64", 2e-6), ("fp32", 1e-3)])
+def test_spectra_files_match_the_reference_post_processor(precision, tol, golden_case):
+    d = golden_case(CASE)
+    r = subprocess.run([str(EXE), "case.cfg", precision, "--spectra"], cwd=d, capture_output=True, text=True,
                        timeout=300)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
-    text = (tmp_path / "case.cfg").read_text()
-    want = spectra.analyse(tmp_path, dt, spectra.source_frequency(text))
-    got = sorted(p.name for p in tmp_path.glob("frequency_slice_*.txt"))
-    assert got == sorted(want) and len(got) == 9
-    for name, (f, k, fs, N, re, im) in want.items():
-        head, rows = spectra.read_frequency_slice(tmp_path / name)
-        assert head[0] == f"# Frequency slice at {f:.3e} Hz (index: {k})"
-        assert head[4] == f"#   Time points: {N}"
-        exp = spectra.expected_rows(spec.nx, spec.ny, re, im)
-        assert rows.shape == exp.shape
-        np.testing.assert_array_equal(rows[:, :2], exp[:, :2])
-        scale = max(float(np.abs(exp[:, 2:4]).max()), 1e-30)
-        # %.6e text against the FFT of the same float32 samples
-        assert float(np.abs(rows[:, 2:4] - exp[:, 2:4]).max()) <= 2e-6 * scale, name
+    want = sorted(p.name for p in (d / "post").glob("frequency_slice_*.txt"))
+    got = sorted(p.name for p in d.glob("frequency_slice_*.txt"))
+    assert got == want and len(got) == 9
+    for name in want:
+        head_ref, rows_ref = spectra.read_frequency_slice(d / "post" / name)
+        head, rows = spectra.read_frequency_slice(d / name)
+        assert head == head_ref, name
+        assert rows.shape == rows_ref.shape
+        np.testing.assert_array_equal(rows[:, :2], rows_ref[:, :2])
+        scale = float(np.abs(rows_ref[:, 2:4]).max())
+        assert float(np.abs(rows[:, 2:4] - rows_ref[:, 2:4]).max()) <= tol * scale, (name, precision)
+
+
+def _crop(a):
+    nx, ny = a.shape
+    return np.array([a[i, j] for i in range(nx) for j in range(ny) if nx * 0.25 < i < nx * 0.75 and ny * 0.25 < j < ny * 0.75])
+
+
+@pytest.mark.parametrize("precision", ["fp64-strict", "fp64"])
+def test_running_dft_matches_the_reference_post_processor(precision, golden_case):
+    d = golden_case(CASE)
+    ref = np.load(d / "spectra.npz")
+    with H.chdir(d):
+        cfg = Config.load("case.cfg")
+        sim = Simulation(cfg.desc(cfg.load_medium(), precision))
+    oi = cfg.output_interval
+    N = (cfg.tsteps - 1) // oi + 1
+    times = [s * oi * cfg.dt for s in range(N)]
+    fs = 1.0 / ((times[-1] - times[0]) / (N - 1))        # frequency_analysis.c:371-373
+    idx = [int(k) for k in ref["index"]]
+    freqs = [k * fs / N for k in idx]                     # frequency_analysis.c:381-390
+    pid = sim.dft_add("Ez", cfg.output_slice_position + 1, freqs, first_step=0, interval=oi, cast_f32=False)
+    sim.step(cfg.tsteps)
+    acc, ns = sim.dft_read(pid)
+    sim.close()
+    assert ns == N
+    worst = 0.0
+    for q in range(len(idx)):
+        got = _crop(acc[q] / N)
+        rows = ref["rows"][q]
+        want = rows[:, 2] + 1j * rows[:, 3]
+        e = H.rel_l2(got, want)
+        worst = max(worst, e)
+        assert e <= 1e-10, (precision, idx[q], e)
+        assert H.rel_l2(got.imag, want.imag) <= 1e-10, (precision, idx[q])
+    print(f"\n{precision} running DFT vs reference post-processor: worst rel L2 {worst:.2e} over {len(idx)} bins")

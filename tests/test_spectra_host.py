@@ -4,6 +4,7 @@ the reference's post-processor as restated in oracle/spectra.py."""
 import ctypes as C
 import math
 
+import numpy as np
 import pytest
 
 from oracle import spectra
@@ -48,3 +49,26 @@ def test_source_frequency_from_cfg(tmp_path):
     assert dt.value == 1.5e-17
     p.write_text("source type=gaussian, x=1\n")
     assert _abi.host_lib().php_spectra_config(str(p).encode(), C.byref(v), C.byref(dt)) != 0
+
+
+def test_numpy_restatement_matches_the_reference_post_processor():
+    """oracle/spectra.py (the NumPy restatement) on the reference's own
+    float32 slices of the spectra_dft case gives the rows the reference's
+    post-processor (frequency_analysis.c, built against the FFTW stand-in)
+    wrote for them: same files, headers and indices, values within the
+    %.6e text precision."""
+    from conftest import GOLDEN
+    d = GOLDEN / "spectra_dft"
+    text = (d / "case.cfg").read_text()
+    dt = float(next(l.split("=", 1)[1] for l in text.splitlines() if l.startswith("dt")))
+    want = spectra.analyse(d / "plain", dt, spectra.source_frequency(text))
+    ref = sorted(p.name for p in (d / "post").glob("frequency_slice_*.txt"))
+    assert sorted(want) == ref and len(ref) == 9
+    for name, (f, k, fs, N, re, im) in want.items():
+        head, rows = spectra.read_frequency_slice(d / "post" / name)
+        assert head[0] == f"# Frequency slice at {f:.3e} Hz (index: {k})"
+        assert head[4] == f"#   Time points: {N}"
+        exp = spectra.expected_rows(re.shape[0], re.shape[1], re, im)
+        np.testing.assert_array_equal(rows[:, :2], exp[:, :2])
+        scale = float(np.abs(exp[:, 2:4]).max())
+        assert float(np.abs(rows[:, 2:4] - exp[:, 2:4]).max()) <= 1e-6 * scale, name
