@@ -35,6 +35,11 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 WORKLOADS = {"cfg0": 0, "cfg1": 1, "cfg2": 2, "cfg3": 3, "cfg4": 4}
+# what the solver computes where the workload texts name parameters the
+# reference's loop has no input for
+REFERENCE_FORM = ("CPML graded as the reference hard-codes it (m = 3, kappa_max = 7, alpha_max = 0.05, "
+                  "fdtd.c:975-977; the cfg0 text names kappa_max = 5); ion equations of motion without a damping "
+                  "term, as fdtd.c:3521-3528 integrate them (the cfg0 text names gamma = 5 cm^-1)")
 
 
 def parse():
@@ -440,6 +445,7 @@ def run_largest(args, local):
             "phase_rms_rad": float(math.sqrt(np.sum(wgt * dphi ** 2) / np.sum(wgt)))}
     return {
         "workload": "cfg4_largest_1024x1024x512", "grid": [cfg.nx, cfg.ny, cfg.nz], "cells": V,
+        "reference_form": REFERENCE_FORM,
         "atom_cells": c["atom_cells"], "ade_cells": c["ade_cells"], "inputs_s": round(t_gen, 1),
         "fp64": out["fp64"], "fp32": out["fp32"],
         "fp32_speedup_vs_fp64": round(out["fp32"]["value"] / out["fp64"]["value"], 3),
@@ -578,7 +584,8 @@ def run_reference_arm(args, ws, rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(res["loop_s"] / steps * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "impl": "reference",
-        "config": {"workload": workload_name(args), "grid": [spec.nx, spec.ny, spec.nz], "cells": V},
+        "config": {"workload": workload_name(args), "grid": [spec.nx, spec.ny, spec.nz], "cells": V,
+                   "reference_form": REFERENCE_FORM},
         "cpu_baseline": {"value": round(rate, 6), "unit": "Gcell-updates/s", "cores": res["ranks"], "kind": "reference",
                          "sample": f"{steps} time steps of the full {spec.nx}x{spec.ny}x{spec.nz} domain, reference "
                                    f"solver ({res['exe']}, -Ofast -funroll-loops, {res['ranks']} MPI ranks as processes "
@@ -678,6 +685,7 @@ def run_serving(args, ws, rank, local):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "impl": "ours",
         "config": {"workload": "cfg3_serving_request stream", "requests": len(reqs), "arrivals": "Poisson 4/s",
+                   "reference_form": REFERENCE_FORM,
                    "edges": "log-uniform 64-192 per axis", "steps": "3000-12000", "pml": 8,
                    "memory_budget_bytes": budget, "max_active": args.max_active, "chunk_steps": 256},
         "latency_s": {"p50": round(float(np.percentile(lat, 50)), 3), "p95": round(float(np.percentile(lat, 95)), 3),
@@ -753,7 +761,8 @@ def main():
             "config": {"workload": workload_name(args), "grid": [cfg.nx, cfg.ny, cfg.nz], "cells": r["V"],
                        "precision": args.precision, "parallelism": f"replicas x{ws}" if ws > 1 else "single domain",
                        "l2": "state 9 fields x cells > L2 (126 MB); no flush needed",
-                       "per_step": "H sweep + fused D/source/E/ADE sweep + monitor probe + running DFT (1 plane)"},
+                       "per_step": "H sweep + fused D/source/E/ADE sweep + monitor probe + running DFT (1 plane)",
+                       "reference_form": REFERENCE_FORM},
             "hbm_gbs": r["roofline"]["achieved"],
             "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": r["e2e"], "clocks": r["clocks"],
             "gpu_launches": r["launches_per_step"] * args.steps,
