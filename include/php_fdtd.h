@@ -188,14 +188,15 @@ int php_step_half(php_ctx* ctx, int32_t half);
  * behind the planes that do not need them (the reference exchanges, then
  * sweeps, fdtd.c:3120-3235).  Parts, enqueued on `stream` (a cudaStream_t;
  * NULL = the context's stream):
- *   0  H sweep of the top z chunk (reads the E halo above); first part of a
- *      step: stages the step's source values and DFT phasors on `stream`
+ *   0  H sweep of the top z chunk (reads the E halo above)
  *   1  H sweep of the other chunks (no halo)
  *   2  fused E sweep of the bottom chunk (reads the H halo below)
  *   3  fused E sweep of the other chunks (no halo)
  *   4  the rest of the step: ion pass, probe, DFT; the step counter advances
- * The caller orders them on the device: 0 before 2, 3 and 4; 1 before 2 and
- * 3 (an E chunk reads H of its own and the plane below); 2 and 3 before 4
+ * The first of parts 0 and 1 called in a step also stages the step's source
+ * values and DFT phasors on its stream.
+ * The caller orders them on the device: 0 and 1 before 2 and 3 (an E chunk
+ * reads H of its own plane and the plane below); 2 and 3 before 4
  * and before the next step's 0 and 1; 4 before the next step's 2 and 3.
  * Parts 0 and 1 may run concurrently, and so may 2 and 3.  With one z chunk
  * parts 1 and 3 launch nothing.  A step must not mix parts with

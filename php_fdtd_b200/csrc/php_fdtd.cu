@@ -39,6 +39,15 @@ constexpr int kMaxChunk = 256;      /* steps per recorded graph */
 constexpr int kProfKinds = 5;       /* H sweep, E sweep, probe, DFT, ion pass */
 constexpr int kProbeCap = 8192;     /* probe rows held on the device */
 constexpr double kEpsInf = 20.0;    /* EPS_INF, fdtd.c:202 */
+/* The FP32 path keeps the lattice state as 2^48 r and 2^48 v: early in a
+ * pulse the reference's displacements are 1e-42 m and below, under FP32's
+ * normal range (1.2e-38), where subnormals keep only a few bits; scaled,
+ * every displacement from 1e-52 m to the 1e-10 m divergence guard is a
+ * normal number.  The factor is folded into QeZM (times 2^48) and QeZV
+ * (times 2^-48), so a = QeZM E - DMM r and P_ion = QeZV r need no extra
+ * operation, and a power of two changes no rounding.  Read-outs multiply
+ * by rv_unit = 2^-48. */
+constexpr double kIonScale32 = 281474976710656.0; /* 2^48 */
 
 thread_local std::string g_create_error; /* errors of php_create, per calling thread */
 
@@ -65,6 +74,7 @@ struct php_ctx {
     int zc_first = 0, zc_count = -1; /* z chunks the sweeps launch over (-1: all) */
     bool part_staged = false;    /* php_step_part: this step's inputs are on the device */
     int num_sms = 148;
+    double rv_unit = 1.0;        /* physical r, v per stored unit (FP32: 2^-48, kIonScale32) */
     bool any_ade = false, any_atoms = false;
     cudaStream_t stream = nullptr;
     /* php_create's own work (allocation, zeroing, uploads) runs on a stream
@@ -698,8 +708,8 @@ static void launch_step_t(php_ctx* ctx, int s_local, int& launches)
         Fields<R> f{fp[0], fp[1], fp[2], fp[3], fp[4], fp[5], fp[6], fp[7], fp[8]};
         const int threads = (9 + 2 * ctx->probe_n3 + 31) / 32 * 32;
         probe_record_counted<R><<<1, threads, 0, ctx->stream>>>(
-            f, ctx->probe_cf, (const R*)ctx->r, (const R*)ctx->v, ctx->nslot, ctx->probe_slot, ctx->probe_n3,
-            ctx->probe_rows, ctx->probe_count, kProbeCap, 9 + 2 * ctx->probe_n3);
+            f, ctx->probe_cf, (const R*)ctx->r, (const R*)ctx->v, ctx->rv_unit, ctx->nslot, ctx->probe_slot,
+            ctx->probe_n3, ctx->probe_rows, ctx->probe_count, kProbeCap, 9 + 2 * ctx->probe_n3);
         prof_mark(ctx, s_local, 2, 1);
         launches++;
     }
@@ -1145,14 +1155,16 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
     std::vector<MatD> mats(d.num_materials);
     std::vector<int> ion_off(d.num_materials, 0);
     std::vector<double> ion_coef;
+    const double ion_scale = ctx->prec == PHP_PREC_FP32 ? kIonScale32 : 1.0;
+    ctx->rv_unit = 1.0 / ion_scale;
     for (int i = 0; i < d.num_materials; i++) {
         int rc = derive_material(ctx, i, d.materials[i], mats[i]);
         if (rc) return rc;
         if (mats[i].natom > 0) {
             const int N = mats[i].natom;
             ion_off[i] = (int)ion_coef.size();
-            ion_coef.insert(ion_coef.end(), d.materials[i].qezv, d.materials[i].qezv + 9 * N);
-            ion_coef.insert(ion_coef.end(), d.materials[i].qezm, d.materials[i].qezm + 9 * N);
+            for (int q = 0; q < 9 * N; q++) ion_coef.push_back(d.materials[i].qezv[q] / ion_scale);
+            for (int q = 0; q < 9 * N; q++) ion_coef.push_back(d.materials[i].qezm[q] * ion_scale);
             ion_coef.insert(ion_coef.end(), d.materials[i].dmm, d.materials[i].dmm + 9 * N * N);
         }
         ctx->mat_natom.push_back(mats[i].natom);
@@ -1207,8 +1219,8 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
             const php_material_desc& M = d.materials[best];
             ctx->ion_k.assign(kIonK, 0.0);
             for (int q = 0; q < 9 * N; q++) {
-                ctx->ion_k[q] = M.qezv[q];
-                ctx->ion_k[kIonKM + q] = M.qezm[q];
+                ctx->ion_k[q] = M.qezv[q] / ion_scale;
+                ctx->ion_k[kIonKM + q] = M.qezm[q] * ion_scale;
             }
             for (int q = 0; q < n3; q++)
                 for (int p = 0; p < n3; p++) ctx->ion_k[kIonKD + q * kIonKQ + p] = M.dmm[(size_t)q * n3 + p];
@@ -1240,11 +1252,14 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
         ctx->nsrc_active++;
     }
 
-    /* z chunking: short marches (8 planes measured best on 256^3, FP64 and
-     * FP32) while keeping at least ~4 waves of blocks on 148 SMs */
+    /* z chunking: short marches while keeping at least ~4 waves of blocks on
+     * 148 SMs.  Measured on 256^3 (the tip workload): FP64 fastest with 4
+     * planes per block (E sweep 0.331 ms, H 0.210 ms; 8 planes 0.339 and
+     * 0.214; 16 planes 0.364 and 0.225), FP32 with 8 (E 0.204 ms; 4 planes
+     * 0.210, 16 planes 0.219) */
     {
         const int tiles = ((nx + kBlockX - 1) / kBlockX) * ((ny + kBlockY - 1) / kBlockY);
-        int zc = std::min(8, nz);
+        int zc = std::min(ctx->prec == PHP_PREC_FP32 ? 8 : 4, nz);
         while (zc > 1 && (int64_t)tiles * ((nz + zc - 1) / zc) < 148 * 4 * 4) zc /= 2;
         ctx->zchunk = d.z_chunk > 0 ? d.z_chunk : zc;
     }
@@ -1612,7 +1627,7 @@ static void launch_frame_gather(php_ctx* ctx, const DiagPartial* fin, int has_po
     R* const* fp = reinterpret_cast<R* const*>(ctx->f);
     Fields<R> f{fp[0], fp[1], fp[2], fp[3], fp[4], fp[5], fp[6], fp[7], fp[8]};
     frame_gather<R><<<1, 256, 0, ctx->stream>>>(f, ctx->mat, ctx->slot, (const MatCoef<R>*)ctx->mc, (const R*)ctx->r,
-                                                 (const R*)ctx->v, ctx->nslot, ctx->nx, ctx->ny, ctx->nz, ctx->nxp,
+                                                 (const R*)ctx->v, ctx->rv_unit, ctx->nslot, ctx->nx, ctx->ny, ctx->nz, ctx->nxp,
                                                  ctx->n3max, fin, has_point, pc, cc,
                                                  ctx->probe ? ctx->probe_count : nullptr, ctx->err_flag,
                                                  ctx->frame_head_dev);
@@ -1718,12 +1733,12 @@ int php_step_part(php_ctx* ctx, int32_t part, void* stream)
     cudaStream_t own = ctx->stream;
     if (stream) ctx->stream = static_cast<cudaStream_t>(stream);
     int rc = PHP_OK;
-    if (part == 0 && !ctx->part_staged) { /* the step's source values and DFT phasors */
+    if (part <= 1 && !ctx->part_staged) { /* the first H part stages the step's source values and DFT phasors */
         rc = stage_step_inputs(ctx, 1, b);
         ctx->part_staged = rc == PHP_OK;
     }
     if (rc == PHP_OK && part != 0 && !ctx->part_staged)
-        rc = fail(ctx, PHP_ERR_STATE, "php_step_part %d before part 0 of the step", part);
+        rc = fail(ctx, PHP_ERR_STATE, "php_step_part %d before an H part (0 or 1) of the step", part);
     if (rc == PHP_OK) {
         ctx->step_in = ctx->step_in_dev[b];
         /* H: part 0 the top chunk, part 1 the others; E: part 2 the bottom
@@ -1940,8 +1955,8 @@ int php_read_cell_state(php_ctx* ctx, int32_t i, int32_t j, int32_t k, int32_t* 
         return PHP_OK;
     };
     for (int q = 0; q < 3 * na; q++) {
-        if (r) { int rc = fetch(ctx->r, q, &r[q]); if (rc) return rc; }
-        if (v) { int rc = fetch(ctx->v, q, &v[q]); if (rc) return rc; }
+        if (r) { int rc = fetch(ctx->r, q, &r[q]); if (rc) return rc; r[q] *= ctx->rv_unit; }
+        if (v) { int rc = fetch(ctx->v, q, &v[q]); if (rc) return rc; v[q] *= ctx->rv_unit; }
     }
     if (ctx->mat_ade[mid] && s >= 0) {
         double pq[3], poq[3];
@@ -2000,13 +2015,13 @@ static int enqueue_diag(php_ctx* ctx, DiagPartial** fin_out)
         float* const* fp = reinterpret_cast<float* const*>(ctx->f);
         Fields<float> f{fp[0], fp[1], fp[2], fp[3], fp[4], fp[5], fp[6], fp[7], fp[8]};
         diag_pass1<float><<<blocks, 256, 0, ctx->stream>>>(f, ctx->nx, ctx->ny, ctx->nz, ctx->nxp, (const float*)ctx->r,
-                                                           ctx->any_atoms ? ctx->nslot : 0, ctx->slot_cell, ctx->slot_n3,
+                                                           ctx->rv_unit, ctx->any_atoms ? ctx->nslot : 0, ctx->slot_cell, ctx->slot_n3,
                                                            std::max(ctx->n3max, 1), part);
     } else {
         double* const* fp = reinterpret_cast<double* const*>(ctx->f);
         Fields<double> f{fp[0], fp[1], fp[2], fp[3], fp[4], fp[5], fp[6], fp[7], fp[8]};
         diag_pass1<double><<<blocks, 256, 0, ctx->stream>>>(f, ctx->nx, ctx->ny, ctx->nz, ctx->nxp, (const double*)ctx->r,
-                                                            ctx->any_atoms ? ctx->nslot : 0, ctx->slot_cell, ctx->slot_n3,
+                                                            ctx->rv_unit, ctx->any_atoms ? ctx->nslot : 0, ctx->slot_cell, ctx->slot_n3,
                                                             std::max(ctx->n3max, 1), part);
     }
     diag_pass2<<<1, 256, 0, ctx->stream>>>(part, blocks, fin);

@@ -246,10 +246,12 @@ __global__ void gather_volume(const R* src, int nx, int ny, int nz, int nxp, dou
 }
 
 /* Probe row appended at count[0]: 9 fields at cf, then r and v of pool slot
- * (3*natom each).  count[1] is raised instead of writing past cap. */
+ * (3*natom each, times rv_unit: the stored state is scaled in FP32).
+ * count[1] is raised instead of writing past cap. */
 template <typename R>
-__global__ void probe_record_counted(const Fields<R> f, int64_t cf, const R* r, const R* v, int64_t nslot,
-                                     int64_t slot, int n3, double* rows, int32_t* count, int cap, int row_len)
+__global__ void probe_record_counted(const Fields<R> f, int64_t cf, const R* r, const R* v, double rv_unit,
+                                     int64_t nslot, int64_t slot, int n3, double* rows, int32_t* count, int cap,
+                                     int row_len)
 {
     __shared__ int row;
     if (threadIdx.x == 0) row = count[0];
@@ -265,7 +267,7 @@ __global__ void probe_record_counted(const Fields<R> f, int64_t cf, const R* r, 
         out[t] = (double)p[t][cf];
     } else if (t < 9 + 2 * n3) {
         const int q = t - 9;
-        out[t] = (q < n3) ? (double)r[(int64_t)q * nslot + slot] : (double)v[(int64_t)(q - n3) * nslot + slot];
+        out[t] = rv_unit * ((q < n3) ? (double)r[(int64_t)q * nslot + slot] : (double)v[(int64_t)(q - n3) * nslot + slot]);
     }
     __syncthreads();
     if (threadIdx.x == 0) count[0] = row + 1;
@@ -313,11 +315,12 @@ __device__ __forceinline__ void diag_merge(DiagPartial& a, const DiagPartial& b)
     }
 }
 
-/* Pass 1 over cells (|E|, |Ex|) and pool slots (|r|); one partial per block
- * into scratch.  slot_cell maps a pool slot to its device cell index. */
+/* Pass 1 over cells (|E|, |Ex|) and pool slots (|r|, times rv_unit); one
+ * partial per block into scratch.  slot_cell maps a pool slot to its device
+ * cell index. */
 template <typename R>
 __global__ void __launch_bounds__(256) diag_pass1(const Fields<R> f, int nx, int ny, int nz, int nxp,
-                                                  const R* r, int64_t nslot, const int64_t* slot_cell,
+                                                  const R* r, double rv_unit, int64_t nslot, const int64_t* slot_cell,
                                                   const int32_t* slot_n3, int n3max, DiagPartial* scratch)
 {
     DiagPartial acc{0.0, 0.0, 0.0, INT64_MAX};
@@ -341,7 +344,7 @@ __global__ void __launch_bounds__(256) diag_pass1(const Fields<R> f, int nx, int
         const int j = (int)(jk % ny), k = (int)(jk / ny);
         const int64_t base = (((int64_t)i * ny + j) * nz + k) * (int64_t)n3max;
         for (int q = 0; q < n3; ++q) {
-            const double rv = fabs((double)r[(int64_t)q * nslot + s]);
+            const double rv = rv_unit * fabs((double)r[(int64_t)q * nslot + s]);
             if (rv > acc.max_r || (rv == acc.max_r && rv > 0.0 && base + q < acc.key_r)) {
                 acc.max_r = rv;
                 acc.key_r = base + q;
@@ -394,9 +397,9 @@ struct FrameHead {
  * atom cell c (none when its material has no atoms). */
 template <typename R>
 __device__ __forceinline__ void frame_cell(const Fields<R>& f, const uint8_t* mat, const int32_t* slot,
-                                           const MatCoef<R>* mc, const R* r, const R* v, int64_t nslot,
-                                           int64_t cf, int64_t ca, double* point9, double* rr, double* vv,
-                                           int32_t* natom)
+                                           const MatCoef<R>* mc, const R* r, const R* v, double rv_unit,
+                                           int64_t nslot, int64_t cf, int64_t ca, double* point9, double* rr,
+                                           double* vv, int32_t* natom)
 {
     const int t = threadIdx.x;
     if (point9 && t < 9) {
@@ -409,8 +412,8 @@ __device__ __forceinline__ void frame_cell(const Fields<R>& f, const uint8_t* ma
     if (t == 0) *natom = s >= 0 ? na : 0;
     if (s < 0) return;
     for (int q = t; q < 3 * na && q < kFrameMaxN3; q += blockDim.x) {
-        rr[q] = (double)r[(int64_t)q * nslot + s];
-        vv[q] = (double)v[(int64_t)q * nslot + s];
+        rr[q] = rv_unit * (double)r[(int64_t)q * nslot + s];
+        vv[q] = rv_unit * (double)v[(int64_t)q * nslot + s];
     }
 }
 
@@ -420,7 +423,8 @@ __device__ __forceinline__ void frame_cell(const Fields<R>& f, const uint8_t* ma
  * (nullptr: no probe).  Thread 0 writes every natom field. */
 template <typename R>
 __global__ void frame_gather(const Fields<R> f, const uint8_t* mat, const int32_t* slot, const MatCoef<R>* mc,
-                             const R* r, const R* v, int64_t nslot, int nx, int ny, int nz, int nxp, int n3max,
+                             const R* r, const R* v, double rv_unit, int64_t nslot, int nx, int ny, int nz, int nxp,
+                             int n3max,
                              const DiagPartial* fin, int has_point, int64_t point_c, int64_t cell_c,
                              const int32_t* probe_count,
                              const int32_t* err, FrameHead* head)
@@ -441,14 +445,16 @@ __global__ void frame_gather(const Fields<R> f, const uint8_t* mat, const int32_
             const int j = (int)(cell % ny);
             const int i = (int)(cell / ny);
             const int64_t c = ((int64_t)k * ny + j) * nxp + i;
-            frame_cell(f, mat, slot, mc, r, v, nslot, c, c, head->diag_point, head->diag_r, head->diag_v, &head->diag_natom);
+            frame_cell(f, mat, slot, mc, r, v, rv_unit, nslot, c, c, head->diag_point, head->diag_r, head->diag_v,
+                       &head->diag_natom);
         }
     }
     if (has_point)
-        frame_cell<R>(f, mat, slot, mc, r, v, nslot, point_c, -1, head->point, nullptr, nullptr, nullptr);
+        frame_cell<R>(f, mat, slot, mc, r, v, rv_unit, nslot, point_c, -1, head->point, nullptr, nullptr, nullptr);
     if (cell_c >= 0) {
         if (t == 0) head->cell_natom = 0;
-        frame_cell<R>(f, mat, slot, mc, r, v, nslot, cell_c, cell_c, nullptr, head->cell_r, head->cell_v, &head->cell_natom);
+        frame_cell<R>(f, mat, slot, mc, r, v, rv_unit, nslot, cell_c, cell_c, nullptr, head->cell_r, head->cell_v,
+                      &head->cell_natom);
     }
     if (t == 0) {
         head->probe_count[0] = probe_count ? probe_count[0] : 0;

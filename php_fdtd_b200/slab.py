@@ -204,6 +204,9 @@ class LocalSlabs:
 
     def close(self):
         self.sync()
+        for st in self._side:
+            st.synchronize()
+        self._p = []
         for s in self.slabs:
             s.close()
 
@@ -214,6 +217,9 @@ class DeviceTransport:
 
     def __init__(self, dist):
         self.dist = dist
+
+    def close(self):
+        pass
 
     def exchange(self, sends, recvs, stream):
         import torch
@@ -235,6 +241,12 @@ class HostTransport:
     def __init__(self, dist):
         self.dist = dist
         self._buf = {}
+
+    def close(self):
+        """Frees the page-locked buffers.  Called while the streams they were
+        copied on still exist: torch's host allocator records an event on
+        each such stream when a buffer is freed."""
+        self._buf.clear()
 
     def _host(self, key, t):
         import torch
@@ -320,5 +332,10 @@ class DistSlab:
         self.slab.sync()
 
     def close(self):
+        """Waits for the slab's work, frees the transport's buffers (their
+        streams must still exist) and the planes' views, then the slab."""
         self.slab.sync()
+        self._side.synchronize()
+        self.transport.close()
+        self._p = {}
         self.slab.close()
