@@ -58,6 +58,7 @@ def parse():
                    help="steps of the FP32-vs-FP64 error run (default: the configuration's tsteps; 0 = skip)")
     p.add_argument("--case-dir", default=None)
     p.add_argument("--no-largest", action="store_true", help="skip the 1024 x 1024 x 512 (cfg4) sub-object")
+    p.add_argument("--no-serving", action="store_true", help="skip the serving (cfg3) sub-object")
     p.add_argument("--z-chunk", type=int, default=0, help="planes per sweep block (0 = the library's choice)")
     p.add_argument("--largest-steps", type=int, default=2000,
                    help="steps of the cfg4 runs whose FP32-vs-FP64 error is reported")
@@ -450,7 +451,36 @@ def run_largest(args, local):
         "fp64": out["fp64"], "fp32": out["fp32"],
         "fp32_speedup_vs_fp64": round(out["fp32"]["value"] / out["fp64"]["value"], 3),
         "error_fp32_vs_fp64": err,
+        "cpu_baseline": largest_reference_sample(case_dir / "case.cfg", cfg.nz, V) if not args.no_cpu_baseline else None,
     }
+
+
+def largest_reference_sample(case_cfg: Path, nz: int, V: int, steps: int = 3):
+    """The reference on the largest domain: a few time steps on every host
+    core (its own loop timer), extrapolated per step.  It needs about 75 GB
+    of host memory (fields, z-psi, per-cell pointer arrays, r/v of 67 M atom
+    cells); skipped with the reason when the host has less."""
+    need = 110 * 10 ** 9
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+    except ImportError:
+        avail = os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
+    if avail < need:
+        return {"value": None, "unit": "Gcell-updates/s", "kind": "reference",
+                "sample": f"skipped: the reference needs about 75 GB of host memory here, {avail / 1e9:.0f} GB available"}
+    ranks = reference_ranks(nz)
+    t0 = time.perf_counter()
+    res, err = reference_rate(case_cfg, steps, ranks, timeout=1500)
+    wall = time.perf_counter() - t0
+    if res is None:
+        return {"value": None, "unit": "Gcell-updates/s", "kind": "reference", "sample": err}
+    return {"value": round(V * steps / res["loop_s"] / 1e9, 6), "unit": "Gcell-updates/s", "cores": res["ranks"],
+            "kind": "reference", "extrapolated": True,
+            "sample": f"{steps} time steps of the full 1024x1024x512 domain, reference solver {res['exe']} "
+                      f"({res['ranks']} MPI ranks as processes through the shared-memory MPI stand-in), its own loop "
+                      f"timer, rate per step extrapolated to the workload; set-up and run {wall:.0f} s wall; "
+                      f"CPU {cpu_model()}"}
 
 
 def accuracy_vs_fp64(args, local, steps: int):
@@ -618,7 +648,11 @@ def run_serving(args, ws, rank, local):
     built = [request_desc(r, "fp32", device=local) for r in reqs]  # host-side inputs, before the clock
     cells = np.array([r["grid"][0] * r["grid"][1] * r["grid"][2] for r in reqs], dtype=np.float64)
     steps = np.array([r["steps"] for r in reqs], dtype=np.float64)
-    sample = sorted(set(np.linspace(0, len(reqs) - 1, min(args.baseline_sample, len(reqs))).round().astype(int).tolist()))
+    # the baseline sample: requests at evenly spaced ranks of their work
+    # (cells x steps), so that it spans the stream's sizes
+    by_work = np.argsort(cells * steps, kind="stable")
+    sample = sorted(set(by_work[np.linspace(0, len(reqs) - 1, min(args.baseline_sample, len(reqs))).round()
+                                .astype(int)].tolist()))
     served = {}
     infos = {}
     done_evt = threading.Event()
@@ -677,6 +711,9 @@ def run_serving(args, ws, rank, local):
     coef, *_ = np.linalg.lstsq(A, np.array(seq_t), rcond=None)
     seq_total = float(np.sum(np.maximum(coef[0] + coef[1] * cs, 0.0)))
     seq_sims_h = len(reqs) / seq_total * 3600.0
+    # the sample itself, timed: its requests one after another in plain FP64
+    sample_sims_h = len(sample) / float(np.sum(seq_t)) * 3600.0
+    sample_work = float(np.mean(cs[sample]) / np.mean(cs))
     h2d = float(np.sum(cells) * 5 + np.sum(steps) * 8 * 4)
     d2h = float(sum(16 * r["grid"][0] * r["grid"][1] for r in reqs))
     line = {
@@ -696,7 +733,12 @@ def run_serving(args, ws, rank, local):
         "makespan_s": round(makespan, 3), "gcell_updates_per_s": round(float(cs.sum()) / makespan / 1e9, 3),
         "failed": len(bad), "server": stats,
         "baseline_sequential_fp64": {"sims_per_h": round(seq_sims_h, 2), "sample": len(sample),
+                                     "method": "the sample's requests run one after another in plain FP64 "
+                                               "(timed); the stream's total from a + b * cells * steps "
+                                               "fitted on them",
                                      "fit_s": [float(coef[0]), float(coef[1])],
+                                     "sample_sims_per_h": round(sample_sims_h, 2),
+                                     "sample_mean_work_vs_stream": round(sample_work, 3),
                                      "speedup": round(sims_h / seq_sims_h, 3)},
         "results": {"identical_to_alone": f"{same}/{len(served)}",
                     "nearfield_rel_l2_vs_fp64_max": round(max(err), 9) if err else None,
@@ -707,8 +749,7 @@ def run_serving(args, ws, rank, local):
         "clocks": clocks.summary(),
         "gpu_launches": int(steps.sum()) * 3,
     }
-    if rank == 0:
-        print(json.dumps(line))
+    return line
 
 
 def main():
@@ -719,7 +760,9 @@ def main():
         barrier(ws)
         return
     if args.workload == "cfg3":
-        run_serving(args, ws, rank, local)
+        line = run_serving(args, ws, rank, local)
+        if rank == 0:
+            print(json.dumps(line))
         barrier(ws)
         return
     sim, cfg, r = run_ours(args, ws, rank, local, args.precision)
@@ -735,9 +778,14 @@ def main():
         acc_steps = args.acc_steps if args.acc_steps is not None else baseline_case(WORKLOADS[args.workload]).tsteps
         if acc_steps > 0 and ws == 1:
             mixed["error_vs_fp64"] = accuracy_vs_fp64(args, local, acc_steps)
-    largest = None
+    largest = serving = None
     if args.precision == "fp64" and args.workload == "cfg1" and args.scale == 1.0 and not args.no_largest:
         largest = run_largest(args, local)
+    if args.precision == "fp64" and args.workload == "cfg1" and ws == 1 and not args.no_serving:
+        sv = run_serving(args, ws, rank, local)
+        serving = {k: sv[k] for k in ("metric", "value", "unit", "latency_s", "makespan_s", "gcell_updates_per_s",
+                                      "failed", "baseline_sequential_fp64", "results", "e2e", "clocks")}
+        serving["config"] = sv["config"]
     if rank == 0:
         cpu = None
         if not args.no_cpu_baseline and ws == 1:
@@ -772,6 +820,8 @@ def main():
             line["mixed"] = mixed
         if largest is not None:
             line["largest"] = largest
+        if serving is not None:
+            line["serving"] = serving
         print(json.dumps(line))
     barrier(ws)
     if ws > 1:
