@@ -779,7 +779,7 @@ def main():
         if acc_steps > 0 and ws == 1:
             mixed["error_vs_fp64"] = accuracy_vs_fp64(args, local, acc_steps)
     largest = serving = None
-    if args.precision == "fp64" and args.workload == "cfg1" and args.scale == 1.0 and not args.no_largest:
+    if args.precision == "fp64" and args.workload == "cfg1" and args.scale == 1.0 and ws == 1 and not args.no_largest:
         largest = run_largest(args, local)
     if args.precision == "fp64" and args.workload == "cfg1" and ws == 1 and not args.no_serving:
         sv = run_serving(args, ws, rank, local)

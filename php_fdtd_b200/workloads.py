@@ -488,8 +488,10 @@ def baseline_case(idx: int, tsteps: Optional[int] = None, seed: int = 0, scale: 
 
 
 # parity cases at the benchmark workloads' own sizes: the full-length
-# config 0, 200-step truncations of configs 1 and 2, and the block-class mix
-PARITY_BASELINE_CASES = ("cfg0_full", "cfg1_200", "cfg2_200", "blocks_mixed")
+# config 0, 200-step truncations of configs 1 and 2, config 4 at half its
+# edge (512 x 512 x 256: its rotated two-atom slab, Drude-Lorentz tip and
+# three-wavenumber source) for 200 steps, and the block-class mix
+PARITY_BASELINE_CASES = ("cfg0_full", "cfg1_200", "cfg2_200", "cfg4_half_200", "blocks_mixed")
 
 
 def parity_baseline_case(name: str) -> CaseSpec:
@@ -499,6 +501,8 @@ def parity_baseline_case(name: str) -> CaseSpec:
         return baseline_case(1, tsteps=200)
     if name == "cfg2_200":
         return baseline_case(2, tsteps=200)
+    if name == "cfg4_half_200":
+        return baseline_case(4, tsteps=200, scale=0.5)
     if name == "blocks_mixed":
         return blocks_mixed_case()
     raise ValueError(f"no baseline parity case {name}")

@@ -45,7 +45,7 @@ from php_fdtd_b200.workloads import (PARITY_BASELINE_CASES, SMALL_CASES, parity_
 import harness as H  # noqa: E402
 
 # reference ranks per baseline case (1 = the one-rank wide build)
-BASELINE_RANKS = {"cfg0_full": 1, "cfg1_200": 1, "cfg2_200": 8, "blocks_mixed": 1}
+BASELINE_RANKS = {"cfg0_full": 1, "cfg1_200": 1, "cfg2_200": 8, "cfg4_half_200": 8, "blocks_mixed": 1}
 
 
 def input_hashes(d: Path) -> dict:
