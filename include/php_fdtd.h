@@ -154,6 +154,11 @@ const char* php_last_error(const php_ctx* ctx);
  * and DFT sample of those steps.  Asynchronous: the work is enqueued on the
  * context's stream (as one CUDA graph per distinct nsteps). */
 int php_step(php_ctx* ctx, int32_t nsteps);
+/* Waits for the context's work.  PHP_ERR_TIMEOUT if a sweep block gave up a
+ * bounded wait for its plane loads (it left after its own loads landed; the
+ * fields of that step are not valid, the context still answers).  With the
+ * environment variable PHP_TEST_STALL_WAIT=1 at php_create, the first block
+ * of every H sweep gives up such a wait on purpose (failure-path tests). */
 int php_sync(php_ctx* ctx);
 int php_get_step(const php_ctx* ctx, int32_t* t);
 /* Records (without running) the CUDA graphs that php_step(ctx, nsteps) will

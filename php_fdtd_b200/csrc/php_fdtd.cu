@@ -75,6 +75,11 @@ struct php_ctx {
     bool part_staged = false;    /* php_step_part: this step's inputs are on the device */
     int num_sms = 148;
     double rv_unit = 1.0;        /* physical r, v per stored unit (FP32: 2^-48, kIonScale32) */
+    /* failure-path test (PHP_TEST_STALL_WAIT=1 at php_create): the first
+     * block of every H sweep gives up a bounded wait on a barrier nothing
+     * arrives on, so the error flag and PHP_ERR_TIMEOUT can be checked
+     * without a fault */
+    int32_t stall_test = 0;
     bool any_ade = false, any_atoms = false;
     cudaStream_t stream = nullptr;
     /* php_create's own work (allocation, zeroing, uploads) runs on a stream
@@ -606,6 +611,7 @@ static StepArgs<R> make_args(php_ctx* ctx, int s_local)
     }
     a.src_val = ctx->step_in + (size_t)s_local * ctx->step_row;
     a.err = ctx->err_flag;
+    a.stall_test = ctx->stall_test;
     return a;
 }
 
@@ -1478,6 +1484,7 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
         ctx->kdp[2] = d.dt / (d.dz * 1.0);
     }
 
+    if (const char* st = getenv("PHP_TEST_STALL_WAIT")) ctx->stall_test = !strcmp(st, "1");
     /* sweep kernels: the TMA plane pipeline */
     if ((rc = dalloc(ctx, (void**)&ctx->err_flag, sizeof(int32_t)))) return rc;
     rc = ctx->prec == PHP_PREC_FP32 ? make_maps<float>(ctx) : make_maps<double>(ctx);

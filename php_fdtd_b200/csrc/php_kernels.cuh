@@ -154,6 +154,7 @@ struct StepArgs {
     int32_t src_comp[kMaxSources];
     const double* src_val;     /* nsrc values of this step */
     int32_t* err;              /* set to 1 by a block whose bounded wait gave up */
+    int32_t stall_test;        /* failure-path test: the first H sweep block's wait gives up */
 };
 
 /* ------------------------------------------------------------ arithmetic */

@@ -119,13 +119,43 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
     return done != 0;
 }
 
-/* bounded wait: false after kWaitLimit polls */
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+/* bounded wait: false after `limit` polls (kWaitLimit by default) */
+__device__ __forceinline__ bool mbar_wait_n(uint64_t* bar, uint32_t parity, uint32_t limit)
 {
-    for (uint32_t n = 0; n < kWaitLimit; ++n)
+    for (uint32_t n = 0; n < limit; ++n)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+{
+    return mbar_wait_n(bar, parity, kWaitLimit);
+}
+
+/* After a bounded wait gave up: waits (bounded again) for the block's plane
+ * loads that may still be in flight -- at most the last S of the `issued`
+ * loads, load g in stage g % S with phase parity (g / S) & 1, since a load
+ * is only issued into a stage whose previous load every thread has
+ * consumed -- so that none lands in shared memory after the block left. */
+__device__ __forceinline__ void ring_drain(uint64_t* full, int S, uint32_t issued)
+{
+    const uint32_t first = issued > (uint32_t)S ? issued - (uint32_t)S : 0u;
+    for (uint32_t g = first; g < issued; ++g) mbar_wait(&full[g % S], (g / S) & 1u);
+}
+
+/* Loads a block has issued when it stops after plane k: the H sweep loads
+ * planes k0..k1 (the first S at once, then plane j + S after plane j), the
+ * fused sweep planes k0-1..k1-1 (then plane j - 1 + S after plane j). */
+__device__ __forceinline__ uint32_t h_loads_issued(int k, int k0, int k1, int S)
+{
+    return (uint32_t)(min(k1, k + S - 1) - k0 + 1);
+}
+__device__ __forceinline__ uint32_t e_loads_issued(int k, int k0, int k1, int S)
+{
+    return (uint32_t)(min(k1 - 1, k + S - 2) - k0 + 2);
+}
+
+/* polls of the failure-path test's wait on a barrier nothing arrives on */
+constexpr uint32_t kStallPolls = 1u << 12;
 
 __device__ __forceinline__ void fence_barrier_init()
 {
@@ -166,7 +196,7 @@ struct TmaGeom {
     static constexpr int ES = sizeof(R) == 8 ? PHP_TMA_ES64 : PHP_TMA_ES32;
     /* dynamic shared memory: 128 bytes of alignment slack, the stages, then
      * the stage barriers */
-    static constexpr uint32_t H_SMEM = 128 + HS * H_STAGE + HS * 8;
+    static constexpr uint32_t H_SMEM = 128 + HS * H_STAGE + (HS + 1) * 8; /* + the failure-path test's barrier */
     /* the fused sweep adds its material records after 128 bytes of barriers:
      * E_SMEM + nmat * sizeof(MatCoef<R>) */
     static constexpr uint32_t E_SMEM = 128 + ES * E_STAGE + 128;
@@ -181,9 +211,11 @@ __device__ __forceinline__ unsigned char* ring_base(unsigned char* dyn)
 
 /* ================================================================ H sweep */
 
-/* fdtd.c:3123-3231: cells i < nx-1, j < ny-1, all k. */
+/* fdtd.c:3123-3231: cells i < nx-1, j < ny-1, all k.  Compiled for the
+ * resident blocks per SM that shared memory allows: six in FP32, four in
+ * FP64. */
 template <typename R, bool STRICT>
-__global__ void __launch_bounds__(kBlockX * kBlockY) h_sweep_tma(const __grid_constant__ StepArgs<R> a,
+__global__ void __launch_bounds__(kBlockX * kBlockY, sizeof(R) == 4 ? 6 : 4) h_sweep_tma(const __grid_constant__ StepArgs<R> a,
                                                                  const __grid_constant__ TmaMaps tm)
 {
     using G = TmaGeom<R>;
@@ -213,12 +245,25 @@ __global__ void __launch_bounds__(kBlockX * kBlockY) h_sweep_tma(const __grid_co
     };
 
     if (tid == 0) {
-        for (int s = 0; s < G::HS; ++s) mbar_init(&full[s], 1);
+        for (int s = 0; s < G::HS + 1; ++s) mbar_init(&full[s], 1);
         fence_barrier_init();
     }
     __syncthreads();
     if (tid == 0)
         for (int p = k0; p <= min(k1, k0 + G::HS - 1); ++p) issue(p);
+    if (a.stall_test && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0) {
+        /* failure-path test (StepArgs::stall_test): a bounded wait on the
+         * barrier after the ring's, on which nothing ever arrives, gives up
+         * like a wait for a plane that never lands */
+        const bool ok = mbar_wait_n(&full[G::HS], 0, kStallPolls);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) {
+                atomicExch(a.err, 1);
+                ring_drain(full, G::HS, h_loads_issued(k0, k0, k1, G::HS));
+            }
+            return;
+        }
+    }
 
     const int eo = ty * G::BX + tx; /* own cell in a halo box */
     const int ho = ty * G::TX + tx; /* own cell in an own box */
@@ -250,7 +295,10 @@ __global__ void __launch_bounds__(kBlockX * kBlockY) h_sweep_tma(const __grid_co
                 a.f.hz[c] = Hs[2 * (HB / sizeof(R)) + ho] + (-khx * dEyx + khy * dExy);
             }
             if (__syncthreads_or(!ok)) {
-                if (tid == 0) atomicExch(a.err, 1);
+                if (tid == 0) {
+                    atomicExch(a.err, 1);
+                    ring_drain(full, G::HS, h_loads_issued(k, k0, k1, G::HS));
+                }
                 break;
             }
             if (tid == 0 && k + G::HS <= k1) {
@@ -399,7 +447,10 @@ __global__ void __launch_bounds__(kBlockX * kBlockY) h_sweep_tma(const __grid_co
         }
         /* every thread is done with plane k: its stage takes plane k + stages */
         if (__syncthreads_or(!ok)) {
-            if (tid == 0) atomicExch(a.err, 1);
+            if (tid == 0) {
+                atomicExch(a.err, 1);
+                ring_drain(full, G::HS, h_loads_issued(k, k0, k1, G::HS));
+            }
             break;
         }
         if (tid == 0 && k + G::HS <= k1) {
@@ -555,7 +606,10 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
                     a.f.ez[c] = ez;
                 }
                 if (__syncthreads_or(!ok)) {
-                    if (tid == 0) atomicExch(a.err, 1);
+                    if (tid == 0) {
+                        atomicExch(a.err, 1);
+                        ring_drain(full, G::ES, e_loads_issued(k, k0, k1, G::ES));
+                    }
                     break;
                 }
                 if (tid == 0 && k - 1 + G::ES <= k1 - 1) {
@@ -639,7 +693,10 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
                 a.f.ez[c] = nc;
             }
             if (__syncthreads_or(!ok)) {
-                if (tid == 0) atomicExch(a.err, 1);
+                if (tid == 0) {
+                    atomicExch(a.err, 1);
+                    ring_drain(full, G::ES, e_loads_issued(k, k0, k1, G::ES));
+                }
                 break;
             }
             if (tid == 0 && k - 1 + G::ES <= k1 - 1) {
@@ -698,7 +755,10 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
                 a.f.ez[c] = iso * dz;
             }
             if (__syncthreads_or(!ok)) {
-                if (tid == 0) atomicExch(a.err, 1);
+                if (tid == 0) {
+                    atomicExch(a.err, 1);
+                    ring_drain(full, G::ES, e_loads_issued(k, k0, k1, G::ES));
+                }
                 break;
             }
             if (tid == 0 && k - 1 + G::ES <= k1 - 1) {
@@ -740,7 +800,10 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
                 a.f.ez[c] = iso * dz;
             }
             if (__syncthreads_or(!ok)) {
-                if (tid == 0) atomicExch(a.err, 1);
+                if (tid == 0) {
+                    atomicExch(a.err, 1);
+                    ring_drain(full, G::ES, e_loads_issued(k, k0, k1, G::ES));
+                }
                 break;
             }
             if (tid == 0 && k - 1 + G::ES <= k1 - 1) {
@@ -804,7 +867,10 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
         }
         /* every thread is done with plane k-1: its stage takes plane k-1 + stages */
         if (__syncthreads_or(!ok)) {
-            if (tid == 0) atomicExch(a.err, 1);
+            if (tid == 0) {
+                atomicExch(a.err, 1);
+                ring_drain(full, G::ES, e_loads_issued(k, k0, k1, G::ES));
+            }
             break;
         }
         if (tid == 0 && k - 1 + G::ES <= k1 - 1) {

@@ -255,6 +255,10 @@ class Simulation:
     def step(self, n: int = 1):
         self._ck(self._lib.php_step(self._ctx, int(n)))
 
+    def prepare(self, n: int):
+        """Records the step graphs of step(n) ahead of its first call (php_prepare)."""
+        self._ck(self._lib.php_prepare(self._ctx, int(n)))
+
     def sync(self):
         self._ck(self._lib.php_sync(self._ctx))
 
