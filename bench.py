@@ -59,6 +59,8 @@ def parse():
     p.add_argument("--case-dir", default=None)
     p.add_argument("--no-largest", action="store_true", help="skip the 1024 x 1024 x 512 (cfg4) sub-object")
     p.add_argument("--no-serving", action="store_true", help="skip the serving (cfg3) sub-object")
+    p.add_argument("--no-configs", action="store_true", help="skip the cfg0 / cfg2 sub-object")
+    p.add_argument("--slabs", type=int, default=0, help="time the workload as this many z slabs on one GPU")
     p.add_argument("--z-chunk", type=int, default=0, help="planes per sweep block (0 = the library's choice)")
     p.add_argument("--largest-steps", type=int, default=2000,
                    help="steps of the cfg4 runs whose FP32-vs-FP64 error is reported")
@@ -201,14 +203,16 @@ def census(cfg, medium: np.ndarray):
             "atom_cells": n_atom_cells, "atom_words": int(atom_words), "pml_e": pml_e, "pml_h": pml_h}
 
 
-def algorithmic_bytes(c: dict, s: int):
+def algorithmic_bytes(c: dict, s: int, ion_pass: bool = False):
     """Compulsory state traffic per launch: H sweep reads E, H and writes H
     (9 words), plus 4 psi words per PML axis; the fused sweep reads H, D and
     writes D, E (12 words), plus old E in lossy/ADE cells (3), P and P_old
-    (12) in ADE cells, r and v (12 N) in atom cells, 4 psi words per PML
-    axis, and the 1-byte material id."""
+    (12) in ADE cells, r and v (12 N) in atom cells -- or, when the ion pass
+    updates the lattice apart, P_ion (3) -- 4 psi words per PML axis, and the
+    1-byte material id."""
     h = s * (9 * c["h_cells"] + 4 * c["pml_h"])
-    e = s * (12 * c["cells"] + 3 * (c["ade_cells"] + c["lossy_cells"]) + 12 * c["ade_cells"] + c["atom_words"]
+    atoms = 3 * c["atom_cells"] if ion_pass else c["atom_words"]
+    e = s * (12 * c["cells"] + 3 * (c["ade_cells"] + c["lossy_cells"]) + 12 * c["ade_cells"] + atoms
              + 4 * c["pml_e"]) + c["cells"]
     return h, e
 
@@ -328,7 +332,7 @@ def run_ours(args, ws, rank, local, precision):
 
     s = 4 if precision == "fp32" else 8
     c = census(cfg, medium)
-    hb, eb = algorithmic_bytes(c, s)
+    hb, eb = algorithmic_bytes(c, s, ion_pass=prof["ion"]["launches"] > 0)
     peaks = {}
     pk = ROOT / "MEASURED_PEAKS.json"
     if pk.exists():
@@ -489,6 +493,77 @@ def largest_reference_sample(case_cfg: Path, nz: int, V: int, steps: int = 3):
                       f"({res['ranks']} MPI ranks as processes through the shared-memory MPI stand-in), its own loop "
                       f"timer, rate per step extrapolated to the workload; set-up and run {wall:.0f} s wall; "
                       f"CPU {cpu_model()}"}
+
+
+def run_other_configs(args, ws, rank, local):
+    """The other single-domain workloads at their full size: config 0 (96^3,
+    two-atom slab) and config 2 (512 x 512 x 256, 16-atom lattice through the
+    ion pass), FP64 and FP32, device-timed over --steps steps; for config 2
+    the ion pass's roofline beside the sweeps'."""
+    import copy
+    out = {}
+    for wl in ("cfg0", "cfg2"):
+        entry = {}
+        for prec in ("fp64", "fp32"):
+            a = copy.copy(args)
+            a.workload, a.no_e2e, a.z_chunk = wl, True, 0
+            sim, cfg, r = run_ours(a, ws, rank, local, prec)
+            sim.close()
+            prof = r["prof"]
+            e = {"value": round(r["value"], 4), "unit": "Gcell-updates/s", "ms_per_step": round(r["ms"] / args.steps, 5),
+                 "kernel_ms": {k: round(v["ms"] / max(1, v["launches"]), 5) for k, v in prof.items() if v["launches"]},
+                 "e_sweep_frac": r["roofline"]["frac"], "h_sweep_frac": r["roofline"]["h_sweep"]["frac"]}
+            c = r["census"]
+            if prof["ion"]["launches"]:
+                s = 4 if prec == "fp32" else 8
+                ion_bytes = s * (c["atom_words"] + 6 * c["atom_cells"]) + 13 * c["atom_cells"]
+                ion_ms = prof["ion"]["ms"] / prof["ion"]["launches"]
+                e["ion_pass"] = {"achieved": round(ion_bytes / (ion_ms * 1e-3) / 1e9, 1), "unit": "GB/s",
+                                 "frac": round(ion_bytes / (ion_ms * 1e-3) / 1e9 / r["roofline"]["peak"], 4),
+                                 "avg_launch_ms": round(ion_ms, 4), "algorithmic_bytes_per_launch": int(ion_bytes)}
+            entry[prec] = e
+        entry["fp32_speedup_vs_fp64"] = round(entry["fp32"]["value"] / entry["fp64"]["value"], 3)
+        from php_fdtd_b200.workloads import CONFIG_NAMES
+        entry["workload"] = CONFIG_NAMES[WORKLOADS[wl]]
+        entry["grid"] = [cfg.nx, cfg.ny, cfg.nz]
+        out[wl] = entry
+    return out
+
+
+def run_slabs(args, local, nslabs: int):
+    """The default workload split into nslabs z slabs on one GPU (LocalSlabs:
+    each step in parts on two streams per slab, halo planes copied device to
+    device, no graphs): wall-clock rate over --steps steps."""
+    import torch
+    from php_fdtd_b200 import Config
+    from php_fdtd_b200.slab import LocalSlabs
+    case_dir = Path(args.case_dir or tempfile.gettempdir()) / f"php_bench_{args.workload}_{args.scale}_slabs"
+    case_dir.mkdir(parents=True, exist_ok=True)
+    make_case(args.workload, args.scale, args.warmup + args.steps + 8, case_dir)
+    old = os.getcwd()
+    os.chdir(case_dir)
+    try:
+        cfg = Config.load("case.cfg")
+        medium = cfg.load_medium()
+    finally:
+        os.chdir(old)
+    holder = cfg.desc(medium, args.precision)
+    holder.desc.device = local
+    slabs = LocalSlabs(holder, nslabs, devices=(local,))
+    slabs.step(args.warmup)
+    slabs.sync()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    slabs.step(args.steps)
+    slabs.sync()
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    slabs.close()
+    V = cfg.nx * cfg.ny * cfg.nz
+    return {"metric": f"Gcell-updates/s, {nslabs} z slabs on one GPU, {args.precision.upper()} path",
+            "value": round(V * args.steps / dt / 1e9, 4), "unit": "Gcell-updates/s", "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 4), "timer": "wall clock",
+            "config": {"workload": workload_name(args), "slabs": [n for _, n in slabs.ranges]}}
 
 
 def accuracy_vs_fp64(args, local, steps: int):
@@ -773,6 +848,9 @@ def main():
             print(json.dumps(line))
         barrier(ws)
         return
+    if args.slabs > 0:
+        print(json.dumps(run_slabs(args, local, args.slabs)))
+        return
     sim, cfg, r = run_ours(args, ws, rank, local, args.precision)
     sim.close()
     mixed = None
@@ -786,7 +864,9 @@ def main():
         acc_steps = args.acc_steps if args.acc_steps is not None else baseline_case(WORKLOADS[args.workload]).tsteps
         if acc_steps > 0 and ws == 1:
             mixed["error_vs_fp64"] = accuracy_vs_fp64(args, local, acc_steps)
-    largest = serving = None
+    largest = serving = configs = None
+    if args.precision == "fp64" and args.workload == "cfg1" and args.scale == 1.0 and ws == 1 and not args.no_configs:
+        configs = run_other_configs(args, ws, rank, local)
     if args.precision == "fp64" and args.workload == "cfg1" and args.scale == 1.0 and ws == 1 and not args.no_largest:
         largest = run_largest(args, local)
     if args.precision == "fp64" and args.workload == "cfg1" and ws == 1 and not args.no_serving:
@@ -830,6 +910,8 @@ def main():
             line["largest"] = largest
         if serving is not None:
             line["serving"] = serving
+        if configs is not None:
+            line["configs"] = configs
         print(json.dumps(line))
     barrier(ws)
     if ws > 1:
