@@ -148,3 +148,30 @@ def test_cfg_defaults_follow_reference_quirks(tmp_path):
     assert s.end_time == cfg.tsteps * cfg.dt
     assert cfg.output_slice_position == 25
     assert cfg.dt == 1e-8 / (3e8 * np.sqrt(3.0)) * 0.99
+
+
+def test_slab_parts_and_census_reject_bad_arguments():
+    lib = _abi.device_lib()
+    counts = (C.c_int64 * 8)()
+    assert lib.php_step_part(None, 0, None) == _abi.PHP_ERR_INPUT
+    assert lib.php_block_census(None, counts) == _abi.PHP_ERR_INPUT
+
+
+def test_bench_bytes_count_p_ion_when_the_ion_pass_runs_apart(golden_case):
+    """bench.py's algorithmic bytes: with the ion pass apart the fused sweep
+    reads P_ion (3 words per atom cell) instead of r and v (12 N words)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_mod", ROOT / "bench.py")
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    d = golden_case("ions16")
+    with H.chdir(d):
+        cfg = Config.load("case.cfg")
+        medium = cfg.load_medium()
+    c = bench.census(cfg, medium)
+    assert c["atom_cells"] == int(np.sum(medium == 10)) and c["atom_words"] == 12 * 16 * c["atom_cells"]
+    for s in (4, 8):
+        h0, e0 = bench.algorithmic_bytes(c, s)
+        h1, e1 = bench.algorithmic_bytes(c, s, ion_pass=True)
+        assert h0 == h1
+        assert e0 - e1 == s * (c["atom_words"] - 3 * c["atom_cells"])
