@@ -217,6 +217,33 @@ def algorithmic_bytes(c: dict, s: int, ion_pass: bool = False):
     return h, e
 
 
+def step_bytes(c: dict, s: int, ion_pass: bool = False):
+    """Compulsory state traffic of the one-launch step (he_sweep_tma): reads E,
+    H, D and writes E, H, D (18 words per cell: H crosses HBM once each way,
+    and the old E of lossy and ADE cells comes with the staged E), P and P_old
+    (12) in ADE cells, r and v (12 N) in atom cells -- or P_ion (3) with the
+    ion pass apart -- 4 psi words per PML axis of the H and of the D update,
+    and the 1-byte material id."""
+    atoms = 3 * c["atom_cells"] if ion_pass else c["atom_words"]
+    return s * (18 * c["cells"] + 12 * c["ade_cells"] + atoms + 4 * (c["pml_h"] + c["pml_e"])) + c["cells"]
+
+
+def sweep_rooflines(prof: dict, c: dict, s: int, peak: float, ion_pass: bool = False) -> dict:
+    """Per-launch rate of each sweep kernel that ran (the one-launch step, or
+    the H sweep and the fused D/E sweep) against the copy bandwidth."""
+    hb, eb = algorithmic_bytes(c, s, ion_pass)
+    out = {}
+    for k, b, name in (("step", step_bytes(c, s, ion_pass), "he_sweep_tma (one-launch step: H, D, sources, E, ADE, ions)"),
+                       ("e_sweep", eb, "e_sweep_tma (fused D/source/E/ADE/ion sweep)"),
+                       ("h_sweep", hb, "h_sweep_tma")):
+        if prof[k]["launches"]:
+            ms = prof[k]["ms"] / prof[k]["launches"]
+            gbs = b / (ms * 1e-3) / 1e9
+            out[k] = {"kernel": name, "achieved": round(gbs, 1), "frac": round(gbs / peak, 4),
+                      "avg_launch_ms": round(ms, 5), "algorithmic_bytes_per_launch": int(b)}
+    return out
+
+
 # ------------------------------------------------------------------ our arm
 
 
@@ -275,7 +302,6 @@ def run_ours(args, ws, rank, local, precision):
     torch.cuda.synchronize()
     barrier(ws)
     ms = ev0.elapsed_time(ev1)
-    launches_per_step = 2 + 1 + 1
     sim.probe_read()
     ms_max = max_over_ranks(ms, ws)
     value = V * args.steps * ws / (ms_max * 1e-3) / 1e9
@@ -332,31 +358,29 @@ def run_ours(args, ws, rank, local, precision):
 
     s = 4 if precision == "fp32" else 8
     c = census(cfg, medium)
-    hb, eb = algorithmic_bytes(c, s, ion_pass=prof["ion"]["launches"] > 0)
     peaks = {}
     pk = ROOT / "MEASURED_PEAKS.json"
     if pk.exists():
         peaks = json.loads(pk.read_text())
     peak = peaks.get("hbm_gbs", 6650.0)
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    e_ms = prof["e_sweep"]["ms"] / max(1, prof["e_sweep"]["launches"])
-    h_ms = prof["h_sweep"]["ms"] / max(1, prof["h_sweep"]["launches"])
-    e_gbs = eb / (e_ms * 1e-3) / 1e9
-    h_gbs = hb / (h_ms * 1e-3) / 1e9
+    sweeps = sweep_rooflines(prof, c, s, peak, ion_pass=prof["ion"]["launches"] > 0)
+    top = "step" if "step" in sweeps else "e_sweep"   # the dominant kernel
     traffic = None
     tf = ROOT / "profiles" / f"traffic_{args.workload}_{precision}.json"
     if tf.exists() and args.scale == 1.0:
-        traffic = json.loads(tf.read_text()).get("e_sweep_dram_bytes_per_launch")
+        traffic = json.loads(tf.read_text()).get(f"{top}_dram_bytes_per_launch")
+    launches_per_step = sum(v["launches"] for v in prof.values()) / max(1, prof[top]["launches"])
     return sim, cfg, {
         "value": value, "ms": ms_max, "V": V, "clocks": clocks.summary(), "prof": prof, "e2e": e2e,
         "launches_per_step": launches_per_step, "census": c, "roofline": {
-            "bound": "hbm", "kernel": "e_sweep (fused D/source/E/ADE/ion sweep)",
-            "achieved": round(e_gbs, 1), "peak": peak, "unit": "GB/s", "frac": round(e_gbs / peak, 4),
+            "bound": "hbm", "kernel": sweeps[top]["kernel"],
+            "achieved": sweeps[top]["achieved"], "peak": peak, "unit": "GB/s", "frac": sweeps[top]["frac"],
             "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured" else "fallback 6650",
-            "traffic": traffic, "algorithmic_bytes_per_launch": eb, "avg_launch_ms": round(e_ms, 5),
-            "h_sweep": {"achieved": round(h_gbs, 1), "frac": round(h_gbs / peak, 4), "avg_launch_ms": round(h_ms, 5),
-                        "algorithmic_bytes_per_launch": hb},
-            "kernel_share": {k: round(v["ms"] / max(1e-9, sum(x["ms"] for x in prof.values())), 4) for k, v in prof.items()}}}
+            "traffic": traffic, "algorithmic_bytes_per_launch": sweeps[top]["algorithmic_bytes_per_launch"],
+            "avg_launch_ms": sweeps[top]["avg_launch_ms"], "sweeps": sweeps,
+            "kernel_share": {k: round(v["ms"] / max(1e-9, sum(x["ms"] for x in prof.values())), 4)
+                             for k, v in prof.items() if v["launches"]}}}
 
 
 def run_largest(args, local):
@@ -430,19 +454,10 @@ def run_largest(args, local):
         census_blocks = sim.block_census()
         sim.close()
         s = 4 if prec == "fp32" else 8
-        hb, eb = algorithmic_bytes(c, s)
-        e_ms = prof["e_sweep"]["ms"] / max(1, prof["e_sweep"]["launches"])
-        h_ms = prof["h_sweep"]["ms"] / max(1, prof["h_sweep"]["launches"])
         out[prec] = {
             "value": round(V * args.steps / (ms * 1e-3) / 1e9, 4), "unit": "Gcell-updates/s",
             "ms_per_step": round(ms / args.steps, 4), "create_s": round(t_create, 2),
-            "roofline": {"bound": "hbm", "peak": peak, "unit": "GB/s",
-                         "e_sweep": {"achieved": round(eb / (e_ms * 1e-3) / 1e9, 1),
-                                     "frac": round(eb / (e_ms * 1e-3) / 1e9 / peak, 4), "avg_launch_ms": round(e_ms, 4),
-                                     "algorithmic_bytes_per_launch": eb},
-                         "h_sweep": {"achieved": round(hb / (h_ms * 1e-3) / 1e9, 1),
-                                     "frac": round(hb / (h_ms * 1e-3) / 1e9 / peak, 4), "avg_launch_ms": round(h_ms, 4),
-                                     "algorithmic_bytes_per_launch": hb}},
+            "roofline": {"bound": "hbm", "peak": peak, "unit": "GB/s", **sweep_rooflines(prof, c, s, peak)},
             "kernel_profile": prof, "blocks": census_blocks, "clocks": clocks.summary()}
     a, b = state["fp32"], state["fp64"]
     err = {"steps": n_total, "reference": "FP64 GPU path (same inputs, same steps)",
@@ -512,7 +527,7 @@ def run_other_configs(args, ws, rank, local):
             prof = r["prof"]
             e = {"value": round(r["value"], 4), "unit": "Gcell-updates/s", "ms_per_step": round(r["ms"] / args.steps, 5),
                  "kernel_ms": {k: round(v["ms"] / max(1, v["launches"]), 5) for k, v in prof.items() if v["launches"]},
-                 "e_sweep_frac": r["roofline"]["frac"], "h_sweep_frac": r["roofline"]["h_sweep"]["frac"]}
+                 **{f"{k}_frac": v["frac"] for k, v in r["roofline"]["sweeps"].items()}}
             c = r["census"]
             if prof["ion"]["launches"]:
                 s = 4 if prec == "fp32" else 8
@@ -830,7 +845,8 @@ def run_serving(args, ws, rank, local):
                 "d2h_bytes_per_step": round(d2h / steps.sum(), 3),
                 "path": "php_batch_submit host descriptions -> php_batch_poll/fetch_dft, whole stream timed"},
         "clocks": clocks.summary(),
-        "gpu_launches": int(steps.sum()) * 3,
+        # per job step: the two sweeps (the one-launch step with PHP_FUSED=1) and the DFT sample
+        "gpu_launches": int(steps.sum()) * (2 if os.environ.get("PHP_FUSED") == "1" else 3),
     }
     return line
 
@@ -897,11 +913,13 @@ def main():
             "config": {"workload": workload_name(args), "grid": [cfg.nx, cfg.ny, cfg.nz], "cells": r["V"],
                        "precision": args.precision, "parallelism": f"replicas x{ws}" if ws > 1 else "single domain",
                        "l2": "state 9 fields x cells > L2 (126 MB); no flush needed",
-                       "per_step": "H sweep + fused D/source/E/ADE sweep + monitor probe + running DFT (1 plane)",
+                       "per_step": ("one-launch step (H, D, sources, E, ADE) + monitor probe + running DFT (1 plane)"
+                                    if "step" in r["roofline"]["sweeps"] else
+                                    "H sweep + fused D/source/E/ADE sweep + monitor probe + running DFT (1 plane)"),
                        "reference_form": REFERENCE_FORM},
             "hbm_gbs": r["roofline"]["achieved"],
             "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": r["e2e"], "clocks": r["clocks"],
-            "gpu_launches": r["launches_per_step"] * args.steps,
+            "gpu_launches": int(round(r["launches_per_step"] * args.steps)),
             "kernel_profile": r["prof"],
         }
         if mixed is not None:

@@ -340,9 +340,11 @@ int php_stream(const php_ctx* ctx, void** stream);
 /* Per-kernel timing.  While enabled, the recorded step graphs carry CUDA
  * events around every sweep kernel and php_step accumulates their device
  * time: ms[0] H sweep, ms[1] fused D/E sweep, ms[2] probe, ms[3] DFT,
- * ms[4] ion pass of many-atom cells, with the number of launches of each in
- * launches[0..4] (both arrays hold 5 entries).  Enabling or disabling resets
- * the sums. */
+ * ms[4] ion pass of many-atom cells, ms[5] the one-launch step (H, D and E
+ * in one sweep, which replaces [0] and [1] where it runs), with the number
+ * of launches of each in launches[] (both arrays hold PHP_PROFILE_KINDS
+ * entries).  Enabling or disabling resets the sums. */
+#define PHP_PROFILE_KINDS 6
 int php_profile_enable(php_ctx* ctx, int32_t enable);
 int php_profile_read(php_ctx* ctx, double* ms, int64_t* launches);
 

@@ -36,7 +36,7 @@ using namespace phpdev;
 namespace {
 
 constexpr int kMaxChunk = 256;      /* steps per recorded graph */
-constexpr int kProfKinds = 5;       /* H sweep, E sweep, probe, DFT, ion pass */
+constexpr int kProfKinds = PHP_PROFILE_KINDS; /* H sweep, E sweep, probe, DFT, ion pass, one-launch step */
 constexpr int kProbeCap = 8192;     /* probe rows held on the device */
 constexpr double kEpsInf = 20.0;    /* EPS_INF, fdtd.c:202 */
 /* The FP32 path keeps the lattice state as 2^48 r and 2^48 v: early in a
@@ -102,6 +102,15 @@ struct php_ctx {
     /* device state */
     void* f[9] = {};            /* field bases (plane 0) */
     void* psi[12] = {};
+    /* one-launch step (he_sweep_tma): the second buffers of E, H (fo[0..2],
+     * fo[6..8]; fo[3..5] = f[3..5]) and of the H CPML state, which the
+     * launch writes the new level to; swap_levels exchanges them with f and
+     * psi after it.  level: how many swaps since php_create, mod 2 */
+    bool fused = false;
+    void* fo[9] = {};
+    void* psio[6] = {};
+    int level = 0;
+    uint8_t* plain_hf = nullptr;  /* StepArgs::plain_hf */
     uint8_t* mat = nullptr;
     uint8_t* plain_blk = nullptr; /* plain blocks of the fused sweep (StepArgs::plain_blk) */
     double kdp[3] = {};
@@ -143,7 +152,7 @@ struct php_ctx {
 
     /* stepping */
     int32_t t = 0;
-    std::map<int, cudaGraphExec_t> graphs; /* key: 2 * steps + input buffer */
+    std::map<int, cudaGraphExec_t> graphs; /* key: 4 * steps + 2 * level + input buffer */
     int last_launches = 0;
 
     /* probe */
@@ -155,8 +164,8 @@ struct php_ctx {
 
     std::vector<DftPlane> dft;
 
-    /* TMA maps of the sweep kernels */
-    TmaMaps maps;
+    /* TMA maps of the sweep kernels; maps_o those of the second buffers */
+    TmaMaps maps, maps_o;
     int64_t census[PHP_CENSUS_LEN] = {}; /* php_block_census */
     int32_t* err_flag = nullptr;
 
@@ -612,7 +621,28 @@ static StepArgs<R> make_args(php_ctx* ctx, int s_local)
     a.src_val = ctx->step_in + (size_t)s_local * ctx->step_row;
     a.err = ctx->err_flag;
     a.stall_test = ctx->stall_test;
+    if (ctx->fused) {
+        for (int q = 0; q < 3; q++) {
+            a.enew[q] = (R*)ctx->fo[PHP_EX + q];
+            a.hnew[q] = (R*)ctx->fo[PHP_HX + q];
+        }
+        for (int q = 0; q < 6; q++) a.psin_h[q] = (R*)ctx->psio[q];
+        a.plain_hf = ctx->plain_hf;
+    }
     return a;
+}
+
+/* After a one-launch step: the buffers it wrote hold the current E, H and H
+ * CPML state (on the host side, for every later launch and read). */
+static void swap_levels(php_ctx* ctx)
+{
+    for (int q = 0; q < 3; q++) {
+        std::swap(ctx->f[PHP_EX + q], ctx->fo[PHP_EX + q]);
+        std::swap(ctx->f[PHP_HX + q], ctx->fo[PHP_HX + q]);
+    }
+    for (int q = 0; q < 6; q++) std::swap(ctx->psi[q], ctx->psio[q]);
+    std::swap(ctx->maps, ctx->maps_o);
+    ctx->level ^= 1;
 }
 
 static inline void prof_mark(php_ctx* ctx, int s_local, int kind, int end)
@@ -685,7 +715,19 @@ static void launch_step_t(php_ctx* ctx, int s_local, int& launches)
     a.zc0 = ctx->zc_count < 0 ? 0 : ctx->zc_first;
     dim3 grid((ctx->nx + kBlockX - 1) / kBlockX, (ctx->ny + kBlockY - 1) / kBlockY,
               ctx->zc_count < 0 ? nchunk : ctx->zc_count);
-    const bool do_h = ctx->step_part & 1, do_e = ctx->step_part & 2, do_rest = ctx->step_part & 4;
+    bool do_h = ctx->step_part & 1, do_e = ctx->step_part & 2;
+    const bool do_rest = ctx->step_part & 4;
+    if constexpr (!STRICT) {
+        if (ctx->fused && do_h && do_e && grid.z > 0) {
+            /* the one-launch step: reads this level, writes the other */
+            prof_mark(ctx, s_local, 5, 0);
+            he_sweep_tma<R, NA><<<grid, block, FusedGeom<R>::SMEM, ctx->stream>>>(a, ctx->maps);
+            prof_mark(ctx, s_local, 5, 1);
+            launches++;
+            swap_levels(ctx);
+            do_h = do_e = false;
+        }
+    }
     if (grid.z == 0) { /* an empty part: no sweep blocks */
     } else if (do_h) {
         prof_mark(ctx, s_local, 0, 0);
@@ -744,6 +786,10 @@ static int prepare_t(php_ctx* ctx)
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(e_sweep_tma<R, STRICT, NA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(TmaGeom<R>::E_SMEM + kSmemMats * sizeof(MatCoef<R>)));
+    if constexpr (!STRICT)
+        if (e == cudaSuccess && ctx->fused)
+            e = cudaFuncSetAttribute(he_sweep_tma<R, NA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)FusedGeom<R>::SMEM);
     if (e != cudaSuccess) return fail(ctx, PHP_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
     return PHP_OK;
 }
@@ -807,15 +853,22 @@ static int make_maps(php_ctx* ctx)
     using G = TmaGeom<R>;
     const CUtensorMapDataType dt = sizeof(R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
     const uint64_t nxp = ctx->nxp, ny = ctx->ny, nzh = ctx->nz + 2;
-    auto base = [&](int q) { return (void*)((char*)ctx->f[q] - (size_t)ctx->plane * sizeof(R)); };
     int rc = PHP_OK;
-    for (int q = 0; q < 3 && !rc; ++q) {
-        rc = encode_map(ctx, &ctx->maps.e_halo[q], base(PHP_EX + q), dt, sizeof(R), nxp, ny, nzh, G::BX, G::BY);
-        if (!rc) rc = encode_map(ctx, &ctx->maps.h_own[q], base(PHP_HX + q), dt, sizeof(R), nxp, ny, nzh, G::TX, G::TY);
-        if (!rc) rc = encode_map(ctx, &ctx->maps.h_halo[q], base(PHP_HX + q), dt, sizeof(R), nxp, ny, nzh, G::BX, G::BY);
-        if (!rc) rc = encode_map(ctx, &ctx->maps.d_own[q], base(PHP_DX + q), dt, sizeof(R), nxp, ny, nzh, G::TX, G::TY);
+    using F = FusedGeom<R>;
+    /* maps of the current buffers, then (one-launch step) of the second ones */
+    for (int set = 0; set < (ctx->fused ? 2 : 1) && !rc; ++set) {
+        TmaMaps& m = set ? ctx->maps_o : ctx->maps;
+        void* const* fb = set ? ctx->fo : ctx->f;
+        auto base = [&](int q) { return (void*)((char*)fb[q] - (size_t)ctx->plane * sizeof(R)); };
+        for (int q = 0; q < 3 && !rc; ++q) {
+            rc = encode_map(ctx, &m.e_halo[q], base(PHP_EX + q), dt, sizeof(R), nxp, ny, nzh, G::BX, G::BY);
+            if (!rc) rc = encode_map(ctx, &m.h_own[q], base(PHP_HX + q), dt, sizeof(R), nxp, ny, nzh, G::TX, G::TY);
+            if (!rc) rc = encode_map(ctx, &m.h_halo[q], base(PHP_HX + q), dt, sizeof(R), nxp, ny, nzh, G::BX, G::BY);
+            if (!rc) rc = encode_map(ctx, &m.d_own[q], base(PHP_DX + q), dt, sizeof(R), nxp, ny, nzh, G::TX, G::TY);
+            if (!rc) rc = encode_map(ctx, &m.e_wide[q], base(PHP_EX + q), dt, sizeof(R), nxp, ny, nzh, F::EX, F::EY);
+        }
+        if (!rc) rc = encode_map(ctx, &m.mat, ctx->mat, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, nxp, ny, ctx->nz, G::TX, G::TY);
     }
-    if (!rc) rc = encode_map(ctx, &ctx->maps.mat, ctx->mat, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, nxp, ny, ctx->nz, G::TX, G::TY);
     return rc;
 }
 
@@ -1335,6 +1388,31 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
         int rc = dalloc(ctx, &ctx->psi[q], psz[q] * rs);
         if (rc) return rc;
     }
+    /* the one-launch step (he_sweep_tma) on a whole domain in the fast
+     * modes, with PHP_FUSED=1 at create: it moves 12 % fewer bytes per step
+     * than the two sweeps but measured slower on B200 (occupancy: E and H
+     * with their halos in the stage ring, 80-125 registers), so the two
+     * sweeps are the default */
+    {
+        const char* fv = getenv("PHP_FUSED");
+        ctx->fused = ctx->prec != PHP_PREC_FP64_STRICT && ctx->z_off == 0 && ctx->nz_glob == nz && fv && !strcmp(fv, "1");
+    }
+    if (ctx->fused) {
+        for (int q = 0; q < 9; q++) {
+            if (q >= PHP_DX && q < PHP_DX + 3) {
+                ctx->fo[q] = ctx->f[q];
+                continue;
+            }
+            void* p;
+            int rc = dalloc(ctx, &p, field_bytes);
+            if (rc) return rc;
+            ctx->fo[q] = (char*)p + (size_t)ctx->plane * rs;
+        }
+        for (int q = 0; q < 6; q++) {
+            int rc = dalloc(ctx, &ctx->psio[q], psz[q] * rs);
+            if (rc) return rc;
+        }
+    }
     int rc = dalloc(ctx, (void**)&ctx->mat, mat_dev.size());
     if (rc) return rc;
     if ((rc = upload(ctx, ctx->mat, mat_dev.data(), mat_dev.size()))) return rc;
@@ -1395,14 +1473,14 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
         const char* pv = getenv("PHP_PLAIN");
         const int gx = (nx + kBlockX - 1) / kBlockX, gy = (ny + kBlockY - 1) / kBlockY;
         const int gz = (nz + ctx->zchunk - 1) / ctx->zchunk;
-        std::vector<uint8_t> pm((size_t)gx * gy * gz, 255), ph(pm.size(), 0);
+        std::vector<uint8_t> pm((size_t)gx * gy * gz, 255), ph(pm.size(), 0), phf(pm.size(), 0);
         std::vector<char> src_tile(pm.size(), 0);
         for (int s = 0; s < ctx->nsrc_active; s++) {
             const int64_t sc = ctx->src_cell[s];
             const int sk = (int)(sc / ctx->plane), sj = (int)((sc % ctx->plane) / nxp), si = (int)(sc % nxp);
             src_tile[((size_t)(sk / ctx->zchunk) * gy + sj / kBlockY) * gx + si / kBlockX] = 1;
         }
-        size_t nplain = 0, nplain_h = 0;
+        size_t nplain = 0, nplain_h = 0, nplain_hf = 0;
         const char* tv = getenv("PHP_PLAIN_TENSOR");
         const bool tns_off = tv && !strcmp(tv, "0");
         /* blocks of the few-atom material when the fused sweep updates its
@@ -1428,6 +1506,16 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
                     if (full && pml_free) { /* the H sweep needs no more */
                         ph[b] = 1;
                         nplain_h++;
+                    }
+                    /* the one-launch step computes H one cell further down in
+                     * x, y and z: those cells must be outside the CPML too */
+                    bool ring_free = pml_free;
+                    if (ring_free && i0 >= 1) ring_free = axes[0].slot[i0 - 1] < 0;
+                    if (ring_free && j0 >= 1) ring_free = axes[1].slot[j0 - 1] < 0;
+                    if (ring_free && k0 >= 1) ring_free = axes[2].slot[k0 - 1] < 0;
+                    if (full && ring_free) {
+                        phf[b] = 1;
+                        nplain_hf++;
                     }
                     if (src_tile[b]) continue;
                     const int id = mat_dev[((size_t)k0 * ny + j0) * nxp + i0];
@@ -1475,6 +1563,10 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
         if (nplain_h) {
             if ((rc = dalloc(ctx, (void**)&ctx->plain_h, ph.size()))) return rc;
             if ((rc = upload(ctx, ctx->plain_h, ph.data(), ph.size()))) return rc;
+        }
+        if (nplain_hf && ctx->fused) {
+            if ((rc = dalloc(ctx, (void**)&ctx->plain_hf, phf.size()))) return rc;
+            if ((rc = upload(ctx, ctx->plain_hf, phf.data(), phf.size()))) return rc;
         }
         ctx->khp[0] = d.dt / (d.mu0 * d.dx * 1.0);
         ctx->khp[1] = d.dt / (d.mu0 * d.dy * 1.0);
@@ -1542,6 +1634,11 @@ static int estimate_bytes(const php_desc& d, uint64_t* out)
     const uint64_t L = d.pml_thickness;
     uint64_t b = 9 * plane * (d.nz + 2) * rs;
     b += 4 * ((uint64_t)d.nz * d.ny * 2 * L + (uint64_t)d.nz * 2 * L * nxp + 2 * L * d.ny * nxp) * rs;
+    const char* fv = getenv("PHP_FUSED");
+    if (d.precision != PHP_PREC_FP64_STRICT && fv && !strcmp(fv, "1")) { /* second E, H and H CPML buffers */
+        b += 6 * plane * (d.nz + 2) * rs;
+        b += 2 * ((uint64_t)d.nz * d.ny * 2 * L + (uint64_t)d.nz * 2 * L * nxp + 2 * L * d.ny * nxp) * rs;
+    }
     b += ncell; /* material ids */
     if (nslot) b += ncell * 4 + nslot * 12;
     if (any_ade) b += 6 * nslot * rs;
@@ -1563,9 +1660,11 @@ static int record_graph(php_ctx* ctx, int n, int b, cudaGraphExec_t* out);
 /* graph of n steps reading per-step input buffer b; a new chunk length
  * records the graphs of both buffers at once, so that a repeated step
  * pattern instantiates nothing after its first pass */
+static int graph_key(const php_ctx* ctx, int n, int b) { return 4 * n + 2 * ctx->level + b; }
+
 static int ensure_graph(php_ctx* ctx, int n, int b, cudaGraphExec_t* out)
 {
-    auto it = ctx->graphs.find(2 * n + b);
+    auto it = ctx->graphs.find(graph_key(ctx, n, b));
     if (it != ctx->graphs.end()) {
         *out = it->second;
         return PHP_OK;
@@ -1576,15 +1675,20 @@ static int ensure_graph(php_ctx* ctx, int n, int b, cudaGraphExec_t* out)
     return record_graph(ctx, n, b, out);
 }
 
+/* The graph of n steps from the current level; each one-launch step of the
+ * recording swaps the levels on the host as the step will on the device, so
+ * the recording ends by restoring the level it started from. */
 static int record_graph(php_ctx* ctx, int n, int b, cudaGraphExec_t* out)
 {
-    const int key = 2 * n + b;
+    const int key = graph_key(ctx, n, b);
+    const int level = ctx->level;
     ctx->step_in = ctx->step_in_dev[b];
     step_fn fn = pick_step(ctx).launch;
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     int launches = 0;
     for (int s = 0; s < n; s++) fn(ctx, s, launches);
+    if (ctx->level != level) swap_levels(ctx);
     cudaError_t le = cudaGetLastError();
     cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
     if (le != cudaSuccess) {
@@ -1844,12 +1948,14 @@ int php_step(php_ctx* ctx, int32_t nsteps)
         rc = ensure_graph(ctx, n, b, &g);
         if (rc) return rc;
         CK(cudaGraphLaunch(g, ctx->stream));
+        if (ctx->fused && (n & 1)) swap_levels(ctx); /* the level the graph leaves current */
         ctx->chunk_no++;
         if (ctx->profile) {
             CK(cudaStreamSynchronize(ctx->stream));
             for (int s = 0; s < n; s++)
                 for (int kind = 0; kind < kProfKinds; kind++) {
-                    if ((kind == 2 && !ctx->probe) || (kind == 3 && ctx->dft.empty()) || (kind == 4 && !ctx->ion_split))
+                    if ((kind == 2 && !ctx->probe) || (kind == 3 && ctx->dft.empty()) || (kind == 4 && !ctx->ion_split) ||
+                        (kind <= 1 && ctx->fused) || (kind == 5 && !ctx->fused))
                         continue;
                     float ms = 0.f;
                     CK(cudaEventElapsedTime(&ms, ctx->prof_ev[((size_t)s * kProfKinds + kind) * 2],
@@ -1858,7 +1964,7 @@ int php_step(php_ctx* ctx, int32_t nsteps)
                     ctx->prof_n[kind] += kind == 3 ? (int64_t)ctx->dft.size() : 1;
                 }
         }
-        ctx->last_launches += n * (2 + (ctx->ion_split ? 1 : 0) + (ctx->probe ? 1 : 0) + (int)ctx->dft.size());
+        ctx->last_launches += n * ((ctx->fused ? 1 : 2) + (ctx->ion_split ? 1 : 0) + (ctx->probe ? 1 : 0) + (int)ctx->dft.size());
         ctx->t += n;
         nsteps -= n;
     }
@@ -1870,12 +1976,16 @@ int php_prepare(php_ctx* ctx, int32_t nsteps)
     if (!ctx) return PHP_ERR_INPUT;
     if (nsteps < 0) return fail(ctx, PHP_ERR_INPUT, "negative step count");
     cudaGraphExec_t g;
-    if (nsteps >= kMaxChunk) {
-        int rc = ensure_graph(ctx, kMaxChunk, 0, &g);
-        if (rc) return rc;
+    /* with the one-launch step, a chunk of odd length leaves the other level
+     * current: the graphs of both levels */
+    int rc = PHP_OK;
+    for (int lv = 0; lv < (ctx->fused ? 2 : 1) && rc == PHP_OK; lv++) {
+        if (lv) swap_levels(ctx);
+        if (nsteps >= kMaxChunk) rc = ensure_graph(ctx, kMaxChunk, 0, &g);
+        if (rc == PHP_OK && nsteps % kMaxChunk) rc = ensure_graph(ctx, nsteps % kMaxChunk, 0, &g);
+        if (lv) swap_levels(ctx);
     }
-    if (nsteps % kMaxChunk) return ensure_graph(ctx, nsteps % kMaxChunk, 0, &g);
-    return PHP_OK;
+    return rc;
 }
 
 int php_sync(php_ctx* ctx)

@@ -155,6 +155,16 @@ struct StepArgs {
     const double* src_val;     /* nsrc values of this step */
     int32_t* err;              /* set to 1 by a block whose bounded wait gave up */
     int32_t stall_test;        /* failure-path test: the first H sweep block's wait gives up */
+    /* the one-launch step (he_sweep_tma): f's E and H and psi's H arrays hold
+     * the old time level, read only during the launch; the new E, H and H
+     * CPML state go to these buffers (D, the D CPML state and the pools are
+     * updated in place) */
+    R *enew[3], *hnew[3];
+    R* psin_h[6];              /* hxy hxz hyx hyz hzx hzy */
+    /* per block of he_sweep_tma: 1 when the H part needs no CPML term and
+     * updates every cell, over the tile, the cells one below it in x and y
+     * and the plane below the z chunk */
+    const uint8_t* plain_hf;
 };
 
 /* ------------------------------------------------------------ arithmetic */
@@ -468,4 +478,5 @@ __global__ void frame_gather(const Fields<R> f, const uint8_t* mat, const int32_
 
 #include "php_sweeps.cuh"
 #include "php_sweeps_tma.cuh"
+#include "php_sweep_fused.cuh"
 #include "php_ions.cuh"

@@ -87,6 +87,7 @@ struct TmaMaps {
     CUtensorMap h_halo[3]; /* Hx, Hy, Hz: box (32 + 16/s) x 9 at (i0 - 16/s, j0 - 1) */
     CUtensorMap d_own[3];  /* Dx, Dy, Dz: box 32 x 8 */
     CUtensorMap mat;       /* uint8 ids (no halo planes): box 32 x 8 */
+    CUtensorMap e_wide[3]; /* Ex, Ey, Ez: box (32 + 32/s) x 10 at (i0 - 16/s, j0 - 1), he_sweep_tma */
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p)

@@ -404,10 +404,10 @@ class Simulation:
         self._ck(self._lib.php_profile_enable(self._ctx, int(bool(enable))))
 
     def profile_read(self) -> dict:
-        ms = np.zeros(5)
-        n = (C.c_int64 * 5)()
+        ms = np.zeros(6)
+        n = (C.c_int64 * 6)()
         self._ck(self._lib.php_profile_read(self._ctx, ms.ctypes.data_as(C.POINTER(C.c_double)), n))
-        names = ("h_sweep", "e_sweep", "probe", "dft", "ion")
+        names = ("h_sweep", "e_sweep", "probe", "dft", "ion", "step")
         return {k: {"ms": float(ms[q]), "launches": int(n[q])} for q, k in enumerate(names)}
 
     @property

@@ -3,8 +3,9 @@
 Every wait of the sweep kernels on a plane load is bounded: after its limit
 the block records an error flag, waits (bounded again) for its own loads
 still in flight and leaves, and the host reports PHP_ERR_TIMEOUT.  With
-PHP_TEST_STALL_WAIT=1 at php_create the first block of every H sweep waits on
-a barrier that nothing ever arrives on, with a short limit: the test checks
+PHP_TEST_STALL_WAIT=1 at php_create the first block of every H sweep (or of
+every one-launch step) waits on a barrier that nothing ever arrives on, with
+a short limit: the test checks
 that the status comes back, that the context still answers, and that a new
 context on the same device steps correctly afterwards.
 """
@@ -25,12 +26,15 @@ def _holder(golden_case, precision):
         return cfg.desc(cfg.load_medium(), precision)
 
 
+@pytest.mark.parametrize("fused", ["1", "0"])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_bounded_wait_gives_up_with_a_timeout_status(precision, golden_case, monkeypatch):
+def test_bounded_wait_gives_up_with_a_timeout_status(precision, fused, golden_case, monkeypatch):
     holder = _holder(golden_case, precision)
     monkeypatch.setenv("PHP_TEST_STALL_WAIT", "1")
+    monkeypatch.setenv("PHP_FUSED", fused)
     stalled = Simulation(holder)
     monkeypatch.delenv("PHP_TEST_STALL_WAIT")
+    monkeypatch.delenv("PHP_FUSED")
     stalled.step(3)
     with pytest.raises(PhpError) as e:
         stalled.sync()
