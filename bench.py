@@ -67,7 +67,64 @@ def parse():
     p.add_argument("--requests", type=int, default=256, help="cfg3: number of requests")
     p.add_argument("--max-active", type=int, default=16, help="cfg3: simulations running at once")
     p.add_argument("--baseline-sample", type=int, default=16, help="cfg3: requests run alone for the baselines")
+    p.add_argument("--concurrency", action="store_true",
+                   help="cfg3 requests of fixed edges, alone and many at once through the serving loop")
     return p.parse_args()
+
+
+def run_concurrency(args, local):
+    """Does running many small simulations at once fill the GPU?  Serving
+    requests (FP32, two-atom slab, tip, 8-cell CPML, running DFT) of a fixed
+    cubic edge: one alone (its own stream, device-timed steps), and N at once
+    through the serving loop (aggregate cell-updates over the makespan on the
+    server clock); against the rate of one 192^3 request alone.  A batched
+    launch over all running jobs could only recover the gap between the
+    concurrent small grids and the large one."""
+    import torch
+    from php_fdtd_b200 import Simulation
+    from php_fdtd_b200.serving import DftSpec, Server
+    from php_fdtd_b200.workloads import request_desc
+
+    def req(edge, steps):
+        return {"index": 0, "arrival": 0.0, "grid": (edge, edge, edge), "pml": 8, "steps": steps,
+                "wavenumber": 1400.0, "tip_height_nm": 20.0}
+
+    def alone(edge, steps):
+        holder, dft = request_desc(req(edge, steps), "fp32", device=local)
+        with Simulation(holder) as sim:
+            sim.dft_add(dft["component"], dft["z_plane"], dft["freqs"])
+            sim.step(64)
+            sim.sync()
+            st = torch.cuda.ExternalStream(sim.stream, device=torch.device("cuda", local))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            sim.step(steps)
+            e1.record(st)
+            e1.synchronize()
+            return edge ** 3 * steps / (e0.elapsed_time(e1) * 1e-3) / 1e9
+
+    def together(edge, steps, n):
+        built = [request_desc(req(edge, steps), "fp32", device=local) for _ in range(n)]
+        with Server(memory_budget=150 * 10 ** 9, device=local, max_active=n) as srv:
+            for q, (holder, dft) in enumerate(built):
+                srv.submit(holder, steps, DftSpec(dft["component"], dft["z_plane"], dft["freqs"]), tag=q)
+            infos = []
+            while len(infos) < n:
+                for info in srv.poll(timeout_ms=200):
+                    infos.append(info)
+                    srv.release(info["job"])
+        bad = sum(i["status"] != 0 for i in infos)
+        # device-busy span: first job started stepping to last job done
+        span = max(i["t_done"] for i in infos) - min(i["t_start"] for i in infos)
+        return n * edge ** 3 * steps / span / 1e9, bad
+
+    out = {"metric": "Gcell-updates/s, serving requests of one edge, FP32", "unit": "Gcell-updates/s",
+           "big_alone": {"edge": 192, "value": round(alone(192, 2000), 3)}, "edges": {}}
+    for edge, steps, n in ((64, 40000, 32), (96, 20000, 24), (128, 10000, 16)):
+        agg, bad = together(edge, steps, n)
+        out["edges"][str(edge)] = {"alone": round(alone(edge, steps), 3), "together": round(agg, 3), "jobs": n,
+                                   "steps": steps, "failed": bad}
+    return out
 
 
 # ----------------------------------------------------------------- plumbing
@@ -866,6 +923,9 @@ def main():
         return
     if args.slabs > 0:
         print(json.dumps(run_slabs(args, local, args.slabs)))
+        return
+    if args.concurrency:
+        print(json.dumps(run_concurrency(args, local)))
         return
     sim, cfg, r = run_ours(args, ws, rank, local, args.precision)
     sim.close()

@@ -1,6 +1,7 @@
 /*
  * php_kernels.cuh -- device types and the small kernels of the PhP_FDTD
- * time step on sm_100a (the two sweeps are in php_sweeps.cuh).
+ * time step on sm_100a (the sweeps are in php_sweeps*.cuh and
+ * php_sweep_fused.cuh, the ion pass in php_ions.cuh).
  *
  * Device layout (one domain per GPU):
  *   field arrays  R[(nz + 2) planes][ny][nxp]   x fastest, nxp = nx rounded up

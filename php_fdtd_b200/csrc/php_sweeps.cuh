@@ -1,6 +1,7 @@
 /*
  * php_sweeps.cuh -- the per-cell physics of one PhP_FDTD time step, shared by
- * the TMA plane-ring sweeps of php_sweeps_tma.cuh:
+ * the TMA plane-ring sweeps of php_sweeps_tma.cuh and the one-launch step of
+ * php_sweep_fused.cuh:
  *
  *   d_update        D += dt (curl H / kappa + psi_D) - eps''  fdtd.c:3238-3356
  *   e_cell_values   D -> E (rotation, eps^-1 or ADE, loss)    fdtd.c:3404-3503
@@ -495,7 +496,7 @@ __device__ __forceinline__ void e_update(const StepArgs<R>& a, const MatCoef<R>&
  * the interior with the lossy eps'' term (fdtd.c:3238-3356), the sources of
  * this step (fdtd.c:3363-3396), D -> E / ADE / ions (fdtd.c:3404-3528).  The
  * new D and E come back in dx..dz and ex_out..ez_out; the caller stores
- * them (e_cell below, or the two-cell sweep with paired stores). */
+ * them (e_cell below in place, he_sweep_tma E into the new level). */
 template <typename R, bool STRICT, int NAMAX>
 __device__ __forceinline__ void e_cell_values(const StepArgs<R>& a, int i, int j, int k, int c, bool interior, int sx,
                                               int sy, R hx0, R hy0, R hz0, R hxk, R hyk, R hz_jm, R hx_jm, R hz_im,

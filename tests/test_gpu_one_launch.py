@@ -121,3 +121,23 @@ def test_probe_and_dft_read_the_new_level(golden_case):
     finally:
         a.close()
         b.close()
+
+
+def test_profile_reports_the_one_launch_step(golden_case):
+    """php_profile_read: the one-launch step under its own kind, no H or E
+    sweep launches; the two sweeps under theirs"""
+    with H.chdir(golden_case("vacuum_pml")):
+        cfg = Config.load("case.cfg")
+        holder = cfg.desc(cfg.load_medium(), "fp32")
+    a, b = _pair(holder)
+    try:
+        for s in (a, b):
+            s.profile(True)
+            s.step(5)
+        pa, pb = a.profile_read(), b.profile_read()
+        assert pa["step"]["launches"] == 5 and pa["h_sweep"]["launches"] == 0 and pa["e_sweep"]["launches"] == 0
+        assert pb["step"]["launches"] == 0 and pb["h_sweep"]["launches"] == 5 and pb["e_sweep"]["launches"] == 5
+        assert pa["step"]["ms"] > 0 and pb["e_sweep"]["ms"] > 0
+    finally:
+        a.close()
+        b.close()
