@@ -285,12 +285,19 @@ def step_bytes(c: dict, s: int, ion_pass: bool = False):
     return s * (18 * c["cells"] + 12 * c["ade_cells"] + atoms + 4 * (c["pml_h"] + c["pml_e"])) + c["cells"]
 
 
-def sweep_rooflines(prof: dict, c: dict, s: int, peak: float, ion_pass: bool = False) -> dict:
+def sweep_rooflines(prof: dict, c: dict, s: int, peak: float, ion_pass: bool = False, dft_cells: int = 0,
+                    dft_freqs: int = 0) -> dict:
     """Per-launch rate of each sweep kernel that ran (the one-launch step, or
-    the H sweep and the fused D/E sweep) against the copy bandwidth."""
+    the H sweep and the fused D/E sweep) against the copy bandwidth.  When no
+    dft_sample launch ran, the E sweep sampled the running DFT itself: per
+    sampled cell the value read back (1 word) and 16 bytes read + 16 written
+    per frequency of its FP64 accumulators."""
     hb, eb = algorithmic_bytes(c, s, ion_pass)
+    dft = dft_cells * (s + 32 * dft_freqs) if prof["dft"]["launches"] == 0 else 0
+    eb += dft
     out = {}
-    for k, b, name in (("step", step_bytes(c, s, ion_pass), "he_sweep_tma (one-launch step: H, D, sources, E, ADE, ions)"),
+    for k, b, name in (("step", step_bytes(c, s, ion_pass) + dft,
+                        "he_sweep_tma (one-launch step: H, D, sources, E, ADE, ions)"),
                        ("e_sweep", eb, "e_sweep_tma (fused D/source/E/ADE/ion sweep)"),
                        ("h_sweep", hb, "h_sweep_tma")):
         if prof[k]["launches"]:
@@ -421,7 +428,7 @@ def run_ours(args, ws, rank, local, precision):
         peaks = json.loads(pk.read_text())
     peak = peaks.get("hbm_gbs", 6650.0)
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    sweeps = sweep_rooflines(prof, c, s, peak, ion_pass=prof["ion"]["launches"] > 0)
+    sweeps = sweep_rooflines(prof, c, s, peak, ion_pass=prof["ion"]["launches"] > 0, dft_cells=nx * ny, dft_freqs=1)
     top = "step" if "step" in sweeps else "e_sweep"   # the dominant kernel
     traffic = None
     tf = ROOT / "profiles" / f"traffic_{args.workload}_{precision}.json"
@@ -514,7 +521,8 @@ def run_largest(args, local):
         out[prec] = {
             "value": round(V * args.steps / (ms * 1e-3) / 1e9, 4), "unit": "Gcell-updates/s",
             "ms_per_step": round(ms / args.steps, 4), "create_s": round(t_create, 2),
-            "roofline": {"bound": "hbm", "peak": peak, "unit": "GB/s", **sweep_rooflines(prof, c, s, peak)},
+            "roofline": {"bound": "hbm", "peak": peak, "unit": "GB/s",
+                         **sweep_rooflines(prof, c, s, peak, dft_cells=cfg.nx * cfg.ny, dft_freqs=len(wn))},
             "kernel_profile": prof, "blocks": census_blocks, "clocks": clocks.summary()}
     a, b = state["fp32"], state["fp64"]
     err = {"steps": n_total, "reference": "FP64 GPU path (same inputs, same steps)",
@@ -902,8 +910,10 @@ def run_serving(args, ws, rank, local):
                 "d2h_bytes_per_step": round(d2h / steps.sum(), 3),
                 "path": "php_batch_submit host descriptions -> php_batch_poll/fetch_dft, whole stream timed"},
         "clocks": clocks.summary(),
-        # per job step: the two sweeps (the one-launch step with PHP_FUSED=1) and the DFT sample
-        "gpu_launches": int(steps.sum()) * (2 if os.environ.get("PHP_FUSED") == "1" else 3),
+        # per job step: the two sweeps (the one-launch step with PHP_FUSED=1), which also sample
+        # the running DFT (a launch of its own with PHP_DFT_FOLD=0)
+        "gpu_launches": int(steps.sum()) * ((1 if os.environ.get("PHP_FUSED") == "1" else 2) +
+                                            (1 if os.environ.get("PHP_DFT_FOLD") == "0" else 0)),
     }
     return line
 

@@ -163,6 +163,9 @@ struct php_ctx {
     int32_t* probe_count = nullptr;
 
     std::vector<DftPlane> dft;
+    /* the E sweep samples E and D planes itself (dft_folded); PHP_DFT_FOLD=0
+     * at create keeps a dft_sample launch per plane */
+    bool dft_fold = true;
 
     /* TMA maps of the sweep kernels; maps_o those of the second buffers */
     TmaMaps maps, maps_o;
@@ -540,6 +543,25 @@ static double source_value(const php_source_desc* s, double time)
 
 /* ------------------------------------------------------------ kernel args */
 
+/* Whether the E sweep samples DFT plane q itself (StepArgs::dft_*): the first
+ * kDftFold planes of E or D components; H planes and the rest take a
+ * dft_sample launch after the step. */
+static bool dft_folded(const php_ctx* ctx, size_t q)
+{
+    if (!ctx->dft_fold || ctx->dft[q].comp > PHP_DZ) return false;
+    int before = 0;
+    for (size_t r = 0; r < q; r++) before += ctx->dft[r].comp <= PHP_DZ;
+    return before < kDftFold;
+}
+
+/* dft_sample launches per step */
+static int dft_launched(const php_ctx* ctx)
+{
+    int n = 0;
+    for (size_t q = 0; q < ctx->dft.size(); q++) n += !dft_folded(ctx, q);
+    return n;
+}
+
 template <typename R>
 static StepArgs<R> make_args(php_ctx* ctx, int s_local)
 {
@@ -621,6 +643,18 @@ static StepArgs<R> make_args(php_ctx* ctx, int s_local)
     a.src_val = ctx->step_in + (size_t)s_local * ctx->step_row;
     a.err = ctx->err_flag;
     a.stall_test = ctx->stall_test;
+    a.ndft = 0;
+    for (size_t q = 0; q < ctx->dft.size(); q++) {
+        if (!dft_folded(ctx, q)) continue;
+        const DftPlane& p = ctx->dft[q];
+        a.dft_z[a.ndft] = p.z;
+        a.dft_comp[a.ndft] = p.comp;
+        a.dft_nfreq[a.ndft] = p.nfreq;
+        a.dft_cast[a.ndft] = p.cast_f32;
+        a.dft_off[a.ndft] = p.in_off;
+        a.dft_acc[a.ndft] = p.acc;
+        a.ndft++;
+    }
     if (ctx->fused) {
         for (int q = 0; q < 3; q++) {
             a.enew[q] = (R*)ctx->fo[PHP_EX + q];
@@ -761,8 +795,11 @@ static void launch_step_t(php_ctx* ctx, int s_local, int& launches)
         prof_mark(ctx, s_local, 2, 1);
         launches++;
     }
-    if (!ctx->dft.empty()) prof_mark(ctx, s_local, 3, 0);
-    for (auto& p : ctx->dft) {
+    const bool dft_kernels = dft_launched(ctx) > 0;
+    if (dft_kernels) prof_mark(ctx, s_local, 3, 0);
+    for (size_t q = 0; q < ctx->dft.size(); q++) {
+        if (dft_folded(ctx, q)) continue; /* sampled by the E sweep */
+        const DftPlane& p = ctx->dft[q];
         R* const* fp = reinterpret_cast<R* const*>(ctx->f);
         const int64_t n = (int64_t)ctx->nx * ctx->ny;
         int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
@@ -771,7 +808,7 @@ static void launch_step_t(php_ctx* ctx, int s_local, int& launches)
                                                        p.in_off, p.in_off + 1, p.acc);
         launches++;
     }
-    if (!ctx->dft.empty()) prof_mark(ctx, s_local, 3, 1);
+    if (dft_kernels) prof_mark(ctx, s_local, 3, 1);
 }
 
 typedef void (*step_fn)(php_ctx*, int, int&);
@@ -1577,6 +1614,7 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
     }
 
     if (const char* st = getenv("PHP_TEST_STALL_WAIT")) ctx->stall_test = !strcmp(st, "1");
+    if (const char* dv = getenv("PHP_DFT_FOLD")) ctx->dft_fold = strcmp(dv, "0") != 0;
     /* sweep kernels: the TMA plane pipeline */
     if ((rc = dalloc(ctx, (void**)&ctx->err_flag, sizeof(int32_t)))) return rc;
     rc = ctx->prec == PHP_PREC_FP32 ? make_maps<float>(ctx) : make_maps<double>(ctx);
@@ -1954,17 +1992,17 @@ int php_step(php_ctx* ctx, int32_t nsteps)
             CK(cudaStreamSynchronize(ctx->stream));
             for (int s = 0; s < n; s++)
                 for (int kind = 0; kind < kProfKinds; kind++) {
-                    if ((kind == 2 && !ctx->probe) || (kind == 3 && ctx->dft.empty()) || (kind == 4 && !ctx->ion_split) ||
+                    if ((kind == 2 && !ctx->probe) || (kind == 3 && dft_launched(ctx) == 0) || (kind == 4 && !ctx->ion_split) ||
                         (kind <= 1 && ctx->fused) || (kind == 5 && !ctx->fused))
                         continue;
                     float ms = 0.f;
                     CK(cudaEventElapsedTime(&ms, ctx->prof_ev[((size_t)s * kProfKinds + kind) * 2],
                                             ctx->prof_ev[((size_t)s * kProfKinds + kind) * 2 + 1]));
                     ctx->prof_ms[kind] += ms;
-                    ctx->prof_n[kind] += kind == 3 ? (int64_t)ctx->dft.size() : 1;
+                    ctx->prof_n[kind] += kind == 3 ? (int64_t)dft_launched(ctx) : 1;
                 }
         }
-        ctx->last_launches += n * ((ctx->fused ? 1 : 2) + (ctx->ion_split ? 1 : 0) + (ctx->probe ? 1 : 0) + (int)ctx->dft.size());
+        ctx->last_launches += n * ((ctx->fused ? 1 : 2) + (ctx->ion_split ? 1 : 0) + (ctx->probe ? 1 : 0) + dft_launched(ctx));
         ctx->t += n;
         nsteps -= n;
     }

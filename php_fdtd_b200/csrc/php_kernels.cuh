@@ -99,6 +99,8 @@ constexpr int kIonKM = 36;
 constexpr int kIonKD = 72;
 constexpr int kIonK = kIonKD + kIonKQ * kIonKQ;
 constexpr int kIsoMats = 32;
+/* running DFT planes the E sweep can sample itself (StepArgs::dft_*) */
+constexpr int kDftFold = 4;
 /* plain-block codes of the fused sweep: id, or kPlainCpml + id for blocks of
  * one plain material with CPML or domain-edge cells, kPlainTensor for blocks
  * of the tensor material in StepArgs::tns_*, kPlainAtoms for blocks of the
@@ -166,6 +168,14 @@ struct StepArgs {
      * updates every cell, over the tile, the cells one below it in x and y
      * and the plane below the z chunk */
     const uint8_t* plain_hf;
+    /* running DFT planes of E or D components that the E sweep samples
+     * after its z march (dft_fold), instead of a dft_sample launch: plane,
+     * component (0-5), frequencies, the float32 cast flag, the offset of the
+     * plane's flag and phasors in the step's input row (src_val), and the
+     * accumulators [nfreq][nx][ny][2] */
+    int32_t ndft;
+    int32_t dft_z[kDftFold], dft_comp[kDftFold], dft_nfreq[kDftFold], dft_cast[kDftFold], dft_off[kDftFold];
+    double* dft_acc[kDftFold];
 };
 
 /* ------------------------------------------------------------ arithmetic */
@@ -285,8 +295,18 @@ __global__ void probe_record_counted(const Fields<R> f, int64_t cf, const R* r, 
     if (threadIdx.x == 0) count[0] = row + 1;
 }
 
-/* Running DFT sample: acc[f][i][j] += x * (cos, sin) for the phasors of this
- * step (phasor[2*f], phasor[2*f+1]); skipped when flag == 0. */
+/* One cell's running-DFT samples: acc[f][t] += x * (cos, sin) for the
+ * phasors of this step (ph[2f], ph[2f+1]), t = i * ny + j of n = nx * ny. */
+__device__ __forceinline__ void dft_accumulate(double x, const double* ph, int nfreq, double* acc, int64_t n, int64_t t)
+{
+    for (int f = 0; f < nfreq; ++f) {
+        double* a = acc + ((int64_t)f * n + t) * 2;
+        a[0] += x * ph[2 * f];
+        a[1] += x * ph[2 * f + 1];
+    }
+}
+
+/* Running DFT sample of one plane; skipped when flag == 0. */
 template <typename R>
 __global__ void dft_sample(const R* src, int64_t plane_off, int nx, int ny, int nxp, int nfreq,
                            int cast_f32, const double* step_in, int flag_off, int phasor_off,
@@ -299,11 +319,29 @@ __global__ void dft_sample(const R* src, int64_t plane_off, int nx, int ny, int 
         const int i = (int)(t / ny), j = (int)(t % ny);
         double x = (double)src[plane_off + (int64_t)j * nxp + i];
         if (cast_f32) x = (double)(float)x;
-        for (int f = 0; f < nfreq; ++f) {
-            double* a = acc + ((int64_t)f * n + t) * 2;
-            a[0] += x * ph[2 * f];
-            a[1] += x * ph[2 * f + 1];
-        }
+        dft_accumulate(x, ph, nfreq, acc, n, t);
+    }
+}
+
+/* The same samples taken by the E sweep (StepArgs::dft_*): after a block's z
+ * march over planes k0 .. k1-1, each of its threads reads back the E or D
+ * values it stored at cell (i, j) of every registered plane in that range
+ * that this step samples (e3: the E arrays the sweep wrote).  A cell's
+ * accumulators belong to the one thread that updates the cell; no register
+ * is held for this inside the march. */
+template <typename R>
+__device__ __forceinline__ void dft_fold(const StepArgs<R>& a, R* const* e3, int i, int j, int k0, int k1)
+{
+    if (i >= a.nx || j >= a.ny) return;
+    for (int q = 0; q < a.ndft; ++q) {
+        const int k = a.dft_z[q];
+        if (k < k0 || k >= k1 || a.src_val[a.dft_off[q]] == 0.0) continue;
+        const int cp = a.dft_comp[q];
+        const R* src = cp == 0 ? e3[0] : cp == 1 ? e3[1] : cp == 2 ? e3[2] : cp == 3 ? a.f.dx : cp == 4 ? a.f.dy : a.f.dz;
+        double x = (double)src[(k * a.ny + j) * a.nxp + i];
+        if (a.dft_cast[q]) x = (double)(float)x;
+        dft_accumulate(x, a.src_val + a.dft_off[q] + 1, a.dft_nfreq[q], a.dft_acc[q], (int64_t)a.nx * a.ny,
+                       (int64_t)i * a.ny + j);
     }
 }
 

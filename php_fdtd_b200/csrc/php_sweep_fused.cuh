@@ -532,6 +532,7 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
         hxk = hx;
         hyk = hy;
     }
+    if (a.ndft) dft_fold(a, a.enew, i, j, k0, k1); /* the new E */
 }
 
 } // namespace phpdev

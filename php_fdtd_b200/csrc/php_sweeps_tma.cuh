@@ -529,6 +529,13 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
 
     const int ho = (ty + 1) * G::BX + tx + G::HALO; /* own cell in a halo box */
     const int oo = ty * G::TX + tx;                 /* own cell in an own box */
+    /* after the march: the running DFT samples of this chunk's planes */
+    auto fold_dft = [&]() {
+        if (a.ndft) {
+            R* const e3[3] = {a.f.ex, a.f.ey, a.f.ez};
+            dft_fold(a, e3, i, j, k0, k1);
+        }
+    };
 
     /* a plain block (one plain isotropic material, no CPML, edge or source
      * cell; marked on the host): D += curl H with the kappa = 1 factors and
@@ -632,6 +639,7 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
                     issue(k - 1 + G::ES);
                 }
             }
+            fold_dft();
             return;
         }
     }
@@ -719,6 +727,7 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
                 issue(k - 1 + G::ES);
             }
         }
+        fold_dft();
         return;
     }
     if (pm != 255 && pm >= kPlainCpml) {
@@ -781,6 +790,7 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
                 issue(k - 1 + G::ES);
             }
         }
+        fold_dft();
         return;
     }
     if (pm != 255) {
@@ -826,6 +836,7 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
                 issue(k - 1 + G::ES);
             }
         }
+        fold_dft();
         return;
     }
 
@@ -893,6 +904,7 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
             issue(k - 1 + G::ES);
         }
     }
+    fold_dft();
 }
 
 } // namespace phpdev

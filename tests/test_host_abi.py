@@ -175,3 +175,27 @@ def test_bench_bytes_count_p_ion_when_the_ion_pass_runs_apart(golden_case):
         h1, e1 = bench.algorithmic_bytes(c, s, ion_pass=True)
         assert h0 == h1
         assert e0 - e1 == s * (c["atom_words"] - 3 * c["atom_cells"])
+
+
+def test_bench_rooflines_count_the_folded_dft(golden_case):
+    """bench.py: with no dft_sample launch the E sweep's bytes include the
+    running DFT it sampled itself (a word read and 32 bytes per frequency of
+    each sampled cell); with the launches they do not."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_mod", ROOT / "bench.py")
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    d = golden_case("ade_metal")
+    with H.chdir(d):
+        cfg = Config.load("case.cfg")
+        medium = cfg.load_medium()
+    c = bench.census(cfg, medium)
+    prof = {k: {"ms": 0.1, "launches": 10} for k in ("h_sweep", "e_sweep", "probe", "dft", "ion")}
+    prof["step"] = {"ms": 0.0, "launches": 0}
+    launched = bench.sweep_rooflines(prof, c, 8, 6500.0, dft_cells=300, dft_freqs=3)
+    prof["dft"]["launches"] = 0
+    folded = bench.sweep_rooflines(prof, c, 8, 6500.0, dft_cells=300, dft_freqs=3)
+    assert set(folded) == {"e_sweep", "h_sweep"}
+    de = folded["e_sweep"]["algorithmic_bytes_per_launch"] - launched["e_sweep"]["algorithmic_bytes_per_launch"]
+    assert de == 300 * (8 + 32 * 3)
+    assert folded["h_sweep"] == launched["h_sweep"]
