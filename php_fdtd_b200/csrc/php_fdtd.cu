@@ -158,14 +158,16 @@ struct php_ctx {
     /* probe */
     bool probe = false;
     int64_t probe_cf = 0, probe_slot = -1;
+    int probe_ka = 0;            /* plane of the atom cell */
     int probe_n3 = 0;
     double* probe_rows = nullptr;
     int32_t* probe_count = nullptr;
 
     std::vector<DftPlane> dft;
     /* the E sweep samples E and D planes itself (dft_folded); PHP_DFT_FOLD=0
-     * at create keeps a dft_sample launch per plane */
-    bool dft_fold = true;
+     * at create keeps a dft_sample launch per plane; likewise it records the
+     * monitor row (probe_folded; PHP_PROBE_FOLD=0) */
+    bool dft_fold = true, probe_fold = true;
 
     /* TMA maps of the sweep kernels; maps_o those of the second buffers */
     TmaMaps maps, maps_o;
@@ -554,6 +556,17 @@ static bool dft_folded(const php_ctx* ctx, size_t q)
     return before < kDftFold;
 }
 
+/* Whether the E sweep records the monitor row itself (StepArgs::probe_*):
+ * the field cell is a plane of the grid (not a halo plane) in the z chunk
+ * of the atom cell, whose r and v that sweep updates (no ion pass apart). */
+static bool probe_folded(const php_ctx* ctx)
+{
+    if (!ctx->probe || !ctx->probe_fold || ctx->ion_split) return false;
+    const int kf = (int)(ctx->probe_cf / ctx->plane);
+    if (ctx->probe_cf < 0 || kf >= ctx->nz) return false;
+    return ctx->probe_n3 == 0 || kf / ctx->zchunk == ctx->probe_ka / ctx->zchunk;
+}
+
 /* dft_sample launches per step */
 static int dft_launched(const php_ctx* ctx)
 {
@@ -655,6 +668,19 @@ static StepArgs<R> make_args(php_ctx* ctx, int s_local)
         a.dft_acc[a.ndft] = p.acc;
         a.ndft++;
     }
+    a.probe_rows = nullptr;
+    if (probe_folded(ctx)) {
+        const int64_t cf = ctx->probe_cf;
+        a.probe_rows = ctx->probe_rows;
+        a.probe_count = ctx->probe_count;
+        a.probe_kf = (int32_t)(cf / ctx->plane);
+        a.probe_j = (int32_t)((cf % ctx->plane) / ctx->nxp);
+        a.probe_i = (int32_t)(cf % ctx->nxp);
+        a.probe_n3 = ctx->probe_n3;
+        a.probe_slot = ctx->probe_slot;
+        a.probe_cap = kProbeCap;
+    }
+    a.rv_unit = ctx->rv_unit;
     if (ctx->fused) {
         for (int q = 0; q < 3; q++) {
             a.enew[q] = (R*)ctx->fo[PHP_EX + q];
@@ -784,7 +810,7 @@ static void launch_step_t(php_ctx* ctx, int s_local, int& launches)
             launches++;
         }
     }
-    if (ctx->probe) {
+    if (ctx->probe && !probe_folded(ctx)) {
         prof_mark(ctx, s_local, 2, 0);
         R* const* fp = reinterpret_cast<R* const*>(ctx->f);
         Fields<R> f{fp[0], fp[1], fp[2], fp[3], fp[4], fp[5], fp[6], fp[7], fp[8]};
@@ -1615,6 +1641,7 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
 
     if (const char* st = getenv("PHP_TEST_STALL_WAIT")) ctx->stall_test = !strcmp(st, "1");
     if (const char* dv = getenv("PHP_DFT_FOLD")) ctx->dft_fold = strcmp(dv, "0") != 0;
+    if (const char* pv = getenv("PHP_PROBE_FOLD")) ctx->probe_fold = strcmp(pv, "0") != 0;
     /* sweep kernels: the TMA plane pipeline */
     if ((rc = dalloc(ctx, (void**)&ctx->err_flag, sizeof(int32_t)))) return rc;
     rc = ctx->prec == PHP_PREC_FP32 ? make_maps<float>(ctx) : make_maps<double>(ctx);
@@ -1992,7 +2019,8 @@ int php_step(php_ctx* ctx, int32_t nsteps)
             CK(cudaStreamSynchronize(ctx->stream));
             for (int s = 0; s < n; s++)
                 for (int kind = 0; kind < kProfKinds; kind++) {
-                    if ((kind == 2 && !ctx->probe) || (kind == 3 && dft_launched(ctx) == 0) || (kind == 4 && !ctx->ion_split) ||
+                    if ((kind == 2 && (!ctx->probe || probe_folded(ctx))) || (kind == 3 && dft_launched(ctx) == 0) ||
+                        (kind == 4 && !ctx->ion_split) ||
                         (kind <= 1 && ctx->fused) || (kind == 5 && !ctx->fused))
                         continue;
                     float ms = 0.f;
@@ -2002,7 +2030,8 @@ int php_step(php_ctx* ctx, int32_t nsteps)
                     ctx->prof_n[kind] += kind == 3 ? (int64_t)dft_launched(ctx) : 1;
                 }
         }
-        ctx->last_launches += n * ((ctx->fused ? 1 : 2) + (ctx->ion_split ? 1 : 0) + (ctx->probe ? 1 : 0) + dft_launched(ctx));
+        ctx->last_launches += n * ((ctx->fused ? 1 : 2) + (ctx->ion_split ? 1 : 0) + (ctx->probe && !probe_folded(ctx) ? 1 : 0) +
+                                   dft_launched(ctx));
         ctx->t += n;
         nsteps -= n;
     }
@@ -2272,6 +2301,7 @@ int php_probe_set(php_ctx* ctx, int32_t i, int32_t j, int32_t k_field, int32_t k
     drop_graphs(ctx);
     ctx->probe_cf = ((int64_t)k_field * ctx->ny + j) * ctx->nxp + i;
     const int64_t ca = ((int64_t)k_atom * ctx->ny + j) * ctx->nxp + i;
+    ctx->probe_ka = k_atom;
     uint8_t mid = 0;
     CK(cudaMemcpy(&mid, ctx->mat + ca, 1, cudaMemcpyDeviceToHost));
     ctx->probe_n3 = 3 * ctx->mat_natom[mid];

@@ -176,6 +176,15 @@ struct StepArgs {
     int32_t ndft;
     int32_t dft_z[kDftFold], dft_comp[kDftFold], dft_nfreq[kDftFold], dft_cast[kDftFold], dft_off[kDftFold];
     double* dft_acc[kDftFold];
+    /* the monitor row the E sweep records after its z march (probe_fold),
+     * instead of a probe_record_counted launch, when the field cell (i, j,
+     * kf) and the atom cell of slot (its r and v updated by the sweep) lie in
+     * one z chunk; probe_rows null: no such row */
+    double* probe_rows;
+    int32_t* probe_count;      /* [rows written, overflow flag] */
+    int32_t probe_i, probe_j, probe_kf, probe_n3, probe_cap;
+    int64_t probe_slot;
+    double rv_unit;            /* physical r, v per stored unit */
 };
 
 /* ------------------------------------------------------------ arithmetic */
@@ -343,6 +352,39 @@ __device__ __forceinline__ void dft_fold(const StepArgs<R>& a, R* const* e3, int
         dft_accumulate(x, a.src_val + a.dft_off[q] + 1, a.dft_nfreq[q], a.dft_acc[q], (int64_t)a.nx * a.ny,
                        (int64_t)i * a.ny + j);
     }
+}
+
+/* The monitor row of probe_record_counted taken by the E sweep
+ * (StepArgs::probe_*): the thread of column (i, j), after its z march over
+ * planes k0 .. k1-1 that hold the field cell, reads back the E and D it
+ * stored there, H (e3, h3: the arrays the step's sweeps wrote), and the r
+ * and v it stored for the atom cell of the same column and chunk.  It is the
+ * one thread of the launch that touches the row counter. */
+template <typename R>
+__device__ __forceinline__ void probe_fold(const StepArgs<R>& a, R* const* e3, R* const* h3, int i, int j, int k0, int k1)
+{
+    if (!a.probe_rows || i != a.probe_i || j != a.probe_j || a.probe_kf < k0 || a.probe_kf >= k1) return;
+    const int row = a.probe_count[0];
+    if (row >= a.probe_cap) {
+        a.probe_count[1] = 1;
+        return;
+    }
+    const int64_t c = ((int64_t)a.probe_kf * a.ny + j) * a.nxp + i;
+    double* out = a.probe_rows + (int64_t)row * (9 + 2 * a.probe_n3);
+    out[0] = (double)e3[0][c];
+    out[1] = (double)e3[1][c];
+    out[2] = (double)e3[2][c];
+    out[3] = (double)a.f.dx[c];
+    out[4] = (double)a.f.dy[c];
+    out[5] = (double)a.f.dz[c];
+    out[6] = (double)h3[0][c];
+    out[7] = (double)h3[1][c];
+    out[8] = (double)h3[2][c];
+    for (int q = 0; q < a.probe_n3; ++q) {
+        out[9 + q] = a.rv_unit * (double)a.r[(int64_t)q * a.nslot + a.probe_slot];
+        out[9 + a.probe_n3 + q] = a.rv_unit * (double)a.v[(int64_t)q * a.nslot + a.probe_slot];
+    }
+    a.probe_count[0] = row + 1;
 }
 
 /* ------------------------------------------------------------ diagnostics */

@@ -533,6 +533,7 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
         hyk = hy;
     }
     if (a.ndft) dft_fold(a, a.enew, i, j, k0, k1); /* the new E */
+    if (a.probe_rows) probe_fold(a, a.enew, a.hnew, i, j, k0, k1);
 }
 
 } // namespace phpdev

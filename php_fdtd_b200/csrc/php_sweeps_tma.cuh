@@ -529,11 +529,14 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
 
     const int ho = (ty + 1) * G::BX + tx + G::HALO; /* own cell in a halo box */
     const int oo = ty * G::TX + tx;                 /* own cell in an own box */
-    /* after the march: the running DFT samples of this chunk's planes */
+    /* after the march: the running DFT samples and the monitor row of this
+     * chunk's planes */
     auto fold_dft = [&]() {
-        if (a.ndft) {
-            R* const e3[3] = {a.f.ex, a.f.ey, a.f.ez};
-            dft_fold(a, e3, i, j, k0, k1);
+        R* const e3[3] = {a.f.ex, a.f.ey, a.f.ez};
+        if (a.ndft) dft_fold(a, e3, i, j, k0, k1);
+        if (a.probe_rows) {
+            R* const h3[3] = {a.f.hx, a.f.hy, a.f.hz};
+            probe_fold(a, e3, h3, i, j, k0, k1);
         }
     };
 

@@ -5,7 +5,8 @@ launches.  Both take the same samples with the same arithmetic, so the
 accumulators must be bit-identical: E and D components, several planes (one
 on a z-chunk boundary), sampling from a later step every few steps, the
 float32 cast, FP64, FP32 and strict, z slabs and the one-launch step.  H
-planes still take the launch.
+planes still take the launch.  The monitor row likewise (PHP_PROBE_FOLD=0
+keeps probe_record_counted) where its field and atom cells share a z chunk.
 """
 import os
 from contextlib import contextmanager
@@ -91,3 +92,49 @@ def test_folded_dft_in_slabs_and_the_one_launch_step(fused, golden_case):
     slabs.close()
     assert ns == launched[0][1]
     np.testing.assert_array_equal(acc, launched[0][0])
+
+
+def _probe_rows(holder, cell, steps, **env):
+    with _env(**env):
+        sim = Simulation(holder)
+    sim.probe_set(*cell)
+    sim.step(steps)
+    rows = sim.probe_read()
+    launches = sim.last_launch_count
+    sim.close()
+    return rows, launches
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp64-strict"])
+@pytest.mark.parametrize("name,kf,ka", [("ions2", 9, 8), ("ions2", 8, 7), ("ade_metal", 5, 5), ("ions2", 16, 15),
+                                        ("ions16", 9, 8)])
+def test_monitor_row_recorded_by_the_sweep_equals_the_probe_launch(name, kf, ka, precision, golden_case):
+    """The monitor row (fields at k_field, r and v at k_atom) recorded by the
+    E sweep after its march equals probe_record_counted's: field and atom cell
+    in one z chunk of 4 planes (recorded by the sweep), in two chunks (8 / 7)
+    and the field cell on the high halo plane (16 of 16; both keep the
+    launch), and the many-atom lattice whose ion pass runs apart (launch)."""
+    with H.chdir(golden_case(name)):
+        cfg = Config.load("case.cfg")
+        holder = cfg.desc(cfg.load_medium(), precision)
+    holder.desc.z_chunk = 4
+    cell = (cfg.nx // 2, cfg.ny // 2, kf, ka)
+    folded, n_f = _probe_rows(holder, cell, 13, PHP_PROBE_FOLD="1")
+    launched, n_l = _probe_rows(holder, cell, 13, PHP_PROBE_FOLD="0")
+    assert folded.shape == launched.shape and folded.shape[0] == 13
+    np.testing.assert_array_equal(folded, launched)
+    # ions16 runs its ion pass apart, except in the strict mode
+    same_chunk = kf < cfg.nz and kf // 4 == ka // 4 and (name != "ions16" or precision == "fp64-strict")
+    assert n_l - n_f == (13 if same_chunk else 0)
+
+
+def test_monitor_row_of_the_one_launch_step(golden_case):
+    with H.chdir(golden_case("ions2")):
+        cfg = Config.load("case.cfg")
+        holder = cfg.desc(cfg.load_medium(), "fp64")
+    holder.desc.z_chunk = 4
+    cell = (cfg.nx // 2, cfg.ny // 2, 9, 8)
+    launched, _ = _probe_rows(holder, cell, 11, PHP_PROBE_FOLD="0")
+    one, n = _probe_rows(holder, cell, 11, PHP_PROBE_FOLD="1", PHP_FUSED="1")
+    np.testing.assert_array_equal(one, launched)
+    assert n == 11  # the one launch per step, nothing else
