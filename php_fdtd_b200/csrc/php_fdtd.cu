@@ -54,7 +54,7 @@ thread_local std::string g_create_error; /* errors of php_create, per calling th
 struct DftPlane {
     int comp, z, first, interval, nfreq, cast_f32;
     std::vector<double> freq;
-    double* acc = nullptr; /* [nfreq][nx][ny][2] */
+    double* acc = nullptr; /* [nfreq][ny][nx][2], x fastest (php_dft_read reorders) */
     int nsamples = 0;
     int in_off = 0;        /* offset of this plane's flag in a step-input row */
 };
@@ -2504,8 +2504,20 @@ int php_dft_read(php_ctx* ctx, int32_t id, double* out, int32_t* nsamples)
     if (!ctx || !out) return PHP_ERR_INPUT;
     if (id < 0 || id >= (int)ctx->dft.size()) return fail(ctx, PHP_ERR_INPUT, "no DFT plane %d", id);
     const DftPlane& p = ctx->dft[id];
-    CK(cudaMemcpyAsync(out, p.acc, (size_t)p.nfreq * ctx->nx * ctx->ny * 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    /* the device keeps [nfreq][ny][nx][2] (x fastest for the samplers);
+     * the caller gets [nfreq][nx][ny][2] */
+    const size_t nx = ctx->nx, ny = ctx->ny;
+    std::vector<double> dev((size_t)p.nfreq * nx * ny * 2);
+    CK(cudaMemcpyAsync(dev.data(), p.acc, dev.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    for (size_t f = 0; f < (size_t)p.nfreq; f++)
+        for (size_t j = 0; j < ny; j++)
+            for (size_t i = 0; i < nx; i++) {
+                const double* src = &dev[((f * ny + j) * nx + i) * 2];
+                double* dst = out + ((f * nx + i) * ny + j) * 2;
+                dst[0] = src[0];
+                dst[1] = src[1];
+            }
     if (nsamples) *nsamples = p.nsamples;
     return PHP_OK;
 }

@@ -172,7 +172,7 @@ struct StepArgs {
      * after its z march (dft_fold), instead of a dft_sample launch: plane,
      * component (0-5), frequencies, the float32 cast flag, the offset of the
      * plane's flag and phasors in the step's input row (src_val), and the
-     * accumulators [nfreq][nx][ny][2] */
+     * accumulators [nfreq][ny][nx][2] */
     int32_t ndft;
     int32_t dft_z[kDftFold], dft_comp[kDftFold], dft_nfreq[kDftFold], dft_cast[kDftFold], dft_off[kDftFold];
     double* dft_acc[kDftFold];
@@ -305,7 +305,9 @@ __global__ void probe_record_counted(const Fields<R> f, int64_t cf, const R* r, 
 }
 
 /* One cell's running-DFT samples: acc[f][t] += x * (cos, sin) for the
- * phasors of this step (ph[2f], ph[2f+1]), t = i * ny + j of n = nx * ny. */
+ * phasors of this step (ph[2f], ph[2f+1]), t = j * nx + i of n = nx * ny
+ * (x fastest, so that a warp's cells along x update adjacent accumulators;
+ * php_dft_read hands them out in [f][i][j] order). */
 __device__ __forceinline__ void dft_accumulate(double x, const double* ph, int nfreq, double* acc, int64_t n, int64_t t)
 {
     for (int f = 0; f < nfreq; ++f) {
@@ -325,7 +327,7 @@ __global__ void dft_sample(const R* src, int64_t plane_off, int nx, int ny, int 
     const int64_t n = (int64_t)nx * ny;
     const double* ph = step_in + phasor_off;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
-        const int i = (int)(t / ny), j = (int)(t % ny);
+        const int j = (int)(t / nx), i = (int)(t % nx);
         double x = (double)src[plane_off + (int64_t)j * nxp + i];
         if (cast_f32) x = (double)(float)x;
         dft_accumulate(x, ph, nfreq, acc, n, t);
@@ -350,7 +352,7 @@ __device__ __forceinline__ void dft_fold(const StepArgs<R>& a, R* const* e3, int
         double x = (double)src[(k * a.ny + j) * a.nxp + i];
         if (a.dft_cast[q]) x = (double)(float)x;
         dft_accumulate(x, a.src_val + a.dft_off[q] + 1, a.dft_nfreq[q], a.dft_acc[q], (int64_t)a.nx * a.ny,
-                       (int64_t)i * a.ny + j);
+                       (int64_t)j * a.nx + i);
     }
 }
 
