@@ -1398,9 +1398,10 @@ static int create_impl(const php_desc* desc, php_ctx* ctx)
     const int namax = n3max / 3;
     ctx->namax_tpl = namax == 0 ? 0 : namax <= 2 ? 2 : namax <= 4 ? 4 : namax <= 8 ? 8 : namax <= 16 ? 16 : 64;
     if (namax > 64) return fail(ctx, PHP_ERR_UNSUPPORTED, "natom %d above the supported 64", namax);
-    /* the FP32 two-atom update indexes its pools with 32-bit offsets */
-    if (ctx->prec == PHP_PREC_FP32 && ctx->namax_tpl == 2 && (uint64_t)ctx->nslot * 6u >= ((uint64_t)1 << 32))
-        return fail(ctx, PHP_ERR_UNSUPPORTED, "%lld atom / ADE cells exceed the 2^32-element pools of the FP32 two-atom update",
+    /* the two-atom update holds r, v in registers and indexes its pools with
+     * 32-bit offsets (both precisions) */
+    if (ctx->namax_tpl == 2 && (uint64_t)ctx->nslot * 6u >= ((uint64_t)1 << 32))
+        return fail(ctx, PHP_ERR_UNSUPPORTED, "%lld atom / ADE cells exceed the 2^32-element pools of the two-atom update",
                     (long long)ctx->nslot);
 
     /* sources */

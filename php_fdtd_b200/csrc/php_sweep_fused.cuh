@@ -313,7 +313,7 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
             if (eph && pm == kPlainAtoms && e_active) {
                 /* the few-atom cell's slot, and its r and v into L1 */
                 constexpr int QN = 3 * NAMAX;
-                constexpr bool VREG = QN * (int)sizeof(R) <= kIonRegBytes;
+                constexpr bool VREG = QN * (int)sizeof(R) <= kIonRegBytesR<R>;
                 const int n3 = 3 * a.amc.natom;
                 ip.slot = a.slot[c];
 #pragma unroll

@@ -221,6 +221,27 @@ __device__ __forceinline__ void d_update(const StepArgs<R>& a, int i, int j, int
  * cell's ion state in registers: 6 FP32 coordinates (two atoms) fit the
  * 64-register budget of the FP32 sweep without spills, FP64 ones do not */
 constexpr int kIonRegBytes = 24;
+/* FP64: the same for two atoms (48 bytes), with the fused sweeps that hold
+ * them compiled for three resident blocks of 80 registers instead of four of
+ * 64 (measured E sweep 1.510 -> 1.464 ms on the 512 x 512 x 256 two-atom
+ * slab, 0.0495 -> 0.0435 ms on the 96^3 one; the 64-register budget would
+ * spill them) */
+#ifndef PHP_ION_REG64
+#define PHP_ION_REG64 48
+#endif
+#ifndef PHP_E_MINBLOCKS64_ATOMS
+#define PHP_E_MINBLOCKS64_ATOMS 3
+#endif
+/* FP32 keeps four blocks of 64 registers for them (three of 80 measured
+ * 0.158 -> 0.171 ms on the 192^3 two-atom grid) */
+#ifndef PHP_E_MINBLOCKS32_ATOMS
+#define PHP_E_MINBLOCKS32_ATOMS 4
+#endif
+template <typename R>
+constexpr int kIonRegBytesR = sizeof(R) == 8 ? PHP_ION_REG64 : kIonRegBytes;
+/* whether the fused update of NAMAX atoms holds a cell's r and v in registers */
+template <typename R, int NAMAX>
+constexpr bool kIonVReg = NAMAX > 0 && 3 * NAMAX * (int)sizeof(R) <= kIonRegBytesR<R>;
 
 /* f(q) for q = 0 .. n3-1 in order; with UNR fully unrolled over the bound
  * QN (predicated), so that arrays indexed by q stay in registers */
@@ -290,7 +311,7 @@ __device__ __forceinline__ void e_update(const StepArgs<R>& a, const MatCoef<R>&
      * few atoms (VREG) r and v of the cell sit in registers and all 2 x 3N
      * loads are issued together here. */
     constexpr int QN = NAMAX > 0 ? 3 * NAMAX : 1;
-    constexpr bool VREG = NAMAX > 0 && QN * (int)sizeof(R) <= kIonRegBytes;
+    constexpr bool VREG = NAMAX > 0 && QN * (int)sizeof(R) <= kIonRegBytesR<R>;
     R pr0 = R(0), pr1 = R(0), pr2 = R(0);
     R rold[QN];
     R vold[VREG ? QN : 1];

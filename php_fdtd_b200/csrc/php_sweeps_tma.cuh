@@ -480,7 +480,10 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, sizeof(R) == 4 ? 6 : 4) h_s
 /* fdtd.c:3238-3528 fused, as e_sweep, with H, D and the material ids
  * streamed through the stage ring. */
 template <typename R, bool STRICT, int NAMAX>
-__global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) == 4 ? PHP_E_MINBLOCKS32 : PHP_E_MINBLOCKS))
+__global__ void __launch_bounds__(kBlockX * kBlockY,
+                                  (NAMAX > 4 ? 1
+                                   : sizeof(R) == 4 ? (kIonVReg<R, NAMAX> ? PHP_E_MINBLOCKS32_ATOMS : PHP_E_MINBLOCKS32)
+                                   : kIonVReg<R, NAMAX> ? PHP_E_MINBLOCKS64_ATOMS : PHP_E_MINBLOCKS))
     e_sweep_tma(const __grid_constant__ StepArgs<R> a, const __grid_constant__ TmaMaps tm)
 {
     using G = TmaGeom<R>;
@@ -555,7 +558,7 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, (NAMAX > 4 ? 1 : sizeof(R) 
              * and v) read before the stage wait */
             const MatCoef<R>& m = a.amc;
             constexpr int QN = 3 * NAMAX;
-            constexpr bool VREG = QN * (int)sizeof(R) <= kIonRegBytes;
+            constexpr bool VREG = QN * (int)sizeof(R) <= kIonRegBytesR<R>;
             const int n3 = 3 * m.natom;
             const bool active = (i < a.nx) && (j < a.ny);
             const bool interior = (i >= 1 && i < a.nx - 1 && j >= 1 && j < a.ny - 1);
