@@ -215,8 +215,11 @@ __device__ __forceinline__ unsigned char* ring_base(unsigned char* dyn)
 /* fdtd.c:3123-3231: cells i < nx-1, j < ny-1, all k.  Compiled for the
  * resident blocks per SM that shared memory allows: six in FP32, four in
  * FP64. */
+#ifndef PHP_H_MINBLOCKS32
+#define PHP_H_MINBLOCKS32 6
+#endif
 template <typename R, bool STRICT>
-__global__ void __launch_bounds__(kBlockX * kBlockY, sizeof(R) == 4 ? 6 : 4) h_sweep_tma(const __grid_constant__ StepArgs<R> a,
+__global__ void __launch_bounds__(kBlockX * kBlockY, sizeof(R) == 4 ? PHP_H_MINBLOCKS32 : 4) h_sweep_tma(const __grid_constant__ StepArgs<R> a,
                                                                  const __grid_constant__ TmaMaps tm)
 {
     using G = TmaGeom<R>;
