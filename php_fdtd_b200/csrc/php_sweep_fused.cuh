@@ -114,8 +114,9 @@ struct HCurl {
 };
 
 /* H of one cell with its CPML terms (the general path of h_sweep_tma):
- * psi holds the old pxy pxz pyx pyz pzx pzy (zero outside the PML); the new
- * ones go to out when out.hxy is set */
+ * psi holds the old pxy pxz pyx pyz pzx pzy (zero outside the PML); with
+ * `store` the new ones go to StepArgs::psin_h (the block's own cells; the
+ * cells below the tile are only read) */
 template <typename R, int EX>
 __device__ __forceinline__ void h_cpml(const StepArgs<R>& a, const HCurl<R, EX>& d, R khx, R khy, R khz, const R* psi,
                                        int sx, int sy, int sz, int i, int j, int k, R& hx, R& hy, R& hz, bool store)
