@@ -48,8 +48,11 @@ constexpr uint32_t kWaitLimit = 1u << 24;
 #ifndef PHP_PSI_EARLY_H64
 #define PHP_PSI_EARLY_H64 1
 #endif
+/* FP32 H sweep: early since its CPML coefficients are loaded once per column
+ * (256^3 tip workload H 0.1223 -> 0.1191 ms, 192^3 two-atom 0.0684 -> 0.0661
+ * ms; before that, late measured faster) */
 #ifndef PHP_PSI_EARLY_H32
-#define PHP_PSI_EARLY_H32 0
+#define PHP_PSI_EARLY_H32 1
 #endif
 /* resident blocks the fused sweep is compiled for (register budget), FP64
  * and FP32 */
@@ -69,6 +72,9 @@ constexpr uint32_t kWaitLimit = 1u << 24;
 #endif
 #ifndef PHP_PSI_AHEAD_E32
 #define PHP_PSI_AHEAD_E32 0
+#endif
+#ifndef PHP_PSI_AHEAD_H32
+#define PHP_PSI_AHEAD_H32 1
 #endif
 /* the general path of the FP32 fused sweep reads pool slots one plane ahead
  * (in FP64 the extra live values spill) */
@@ -355,7 +361,7 @@ __global__ void __launch_bounds__(kBlockX * kBlockY, sizeof(R) == 4 ? PHP_H_MINB
             }
         };
         if constexpr (early) load_psi();
-        if (PHP_PSI_AHEAD && !STRICT && active && k + 1 < k1) {
+        if (PHP_PSI_AHEAD && (sizeof(R) == 8 || PHP_PSI_AHEAD_H32) && !STRICT && active && k + 1 < k1) {
             /* the lines of plane k + 1 requested into L1 a plane ahead */
             const int sz1 = ldg_nh(a.tz.slot + k + 1);
             if (sx >= 0) {
